@@ -1,0 +1,840 @@
+// Host side of the C ABI declared in include/godunov2d.h.
+//
+// gd2d_setup validates the reference-layout meshes, reorders cells and
+// nodes along a Hilbert curve (or keeps the natural order), concatenates
+// all cases with per-case padding so that no tile of the cell kernel spans
+// two cases, and uploads the packed layout.  The permutation is kept with
+// its exact inverse so that every download is in reference order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/godunov2d.h"
+#include "gd2d_internal.h"
+
+using namespace gd2d;
+
+namespace {
+
+thread_local std::string g_setup_error;
+
+struct HostCase {
+    int64_t nc = 0, nn = 0, nc_pad = 0;
+    int64_t cell_off = 0, node_off = 0;
+    std::vector<int64_t> cell_perm, cell_inv;  // perm[new] = old, inv[old] = new
+    std::vector<int64_t> node_perm, node_inv;
+    gd2d_params params{};
+    double start_time = 0.0;
+    bool state_set = false;
+};
+
+struct DevBuffers {
+    std::vector<void *> all;
+    template <class T>
+    cudaError_t alloc(T **p, size_t count) {
+        *p = nullptr;
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+        if (e == cudaSuccess) {
+            all.push_back(*p);
+            e = cudaMemset(*p, 0, count * sizeof(T));
+        }
+        return e;
+    }
+    void free_all() {
+        for (void *p : all) cudaFree(p);
+        all.clear();
+    }
+};
+
+}  // namespace
+
+struct gd2d_handle {
+    int device = 0;
+    int32_t ncases = 0;
+    std::vector<HostCase> cases;
+    gd2d_launch launch{};
+    LaunchCfg lc{};
+    int flux = FLUX_AUSM;
+    bool visc = false, quads = false, tgv = false, mixed = false;
+    DevMesh m{};
+    DevState s{};
+    DevBuffers buf;
+    std::vector<DevCase> hcases;
+    std::vector<int32_t> tile_case_h;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    bool state_ready = false;
+    std::vector<std::vector<gd2d_stats>> history;
+    std::vector<cudaEvent_t> ev;  // pairs around cell kernels of the captured graph
+    cudaEvent_t ev_total[2] = {nullptr, nullptr};
+    double last_total_ms = 0.0, last_cell_ms = 0.0;
+    int64_t last_launches = 0;
+    std::string err;
+};
+
+namespace {
+
+int fail(gd2d_handle *h, int code, const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf;
+    else g_setup_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(h, call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e__ = (call);                                                                  \
+        if (e__ != cudaSuccess)                                                                    \
+            return fail((h), e__ == cudaErrorMemoryAllocation ? GD2D_ERR_OOM : GD2D_ERR_CUDA,      \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e__), __FILE__, __LINE__);     \
+    } while (0)
+
+inline int64_t cidx(int64_t n, int64_t i, int64_t j) { return i + j * n; }
+
+// Hilbert index of (x, y) on a 2^16 grid (Butz / Lam-Shapiro iterative form).
+uint64_t hilbert_index(uint32_t x, uint32_t y) {
+    const uint32_t n = 1u << 16;
+    uint64_t d = 0;
+    for (uint32_t s = n / 2; s > 0; s /= 2) {
+        uint32_t rx = (x & s) ? 1u : 0u;
+        uint32_t ry = (y & s) ? 1u : 0u;
+        d += (uint64_t)s * (uint64_t)s * (uint64_t)((3u * rx) ^ ry);
+        if (ry == 0) {
+            if (rx == 1) {
+                x = n - 1 - x;
+                y = n - 1 - y;
+            }
+            std::swap(x, y);
+        }
+    }
+    return d;
+}
+
+void hilbert_order(const std::vector<double> &xs, const std::vector<double> &ys, std::vector<int64_t> &perm) {
+    const size_t n = xs.size();
+    double x0 = INFINITY, x1 = -INFINITY, y0 = INFINITY, y1 = -INFINITY;
+    for (size_t i = 0; i < n; ++i) {
+        x0 = std::min(x0, xs[i]); x1 = std::max(x1, xs[i]);
+        y0 = std::min(y0, ys[i]); y1 = std::max(y1, ys[i]);
+    }
+    double span = std::max(x1 - x0, y1 - y0);
+    if (!(span > 0)) span = 1.0;
+    std::vector<uint64_t> key(n);
+    for (size_t i = 0; i < n; ++i) {
+        uint32_t qx = (uint32_t)std::min(65535.0, std::floor((xs[i] - x0) / span * 65535.0));
+        uint32_t qy = (uint32_t)std::min(65535.0, std::floor((ys[i] - y0) / span * 65535.0));
+        key[i] = hilbert_index(qx, qy);
+    }
+    perm.resize(n);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::stable_sort(perm.begin(), perm.end(), [&](int64_t a, int64_t b) { return key[a] < key[b]; });
+}
+
+// Reverse Cuthill-McKee over the face-neighbour graph of the cells.
+void rcm_order(const gd2d_mesh_view &mv, std::vector<int64_t> &perm) {
+    const int64_t n = mv.n_cells;
+    std::vector<int> deg(n, 0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int k = 0; k < 4; ++k) if (mv.cell_stiffness[cidx(n, i, k)] >= 1) ++deg[i];
+    std::vector<char> seen(n, 0);
+    std::vector<int64_t> order;
+    order.reserve(n);
+    std::vector<int64_t> byd(n);
+    std::iota(byd.begin(), byd.end(), 0);
+    std::stable_sort(byd.begin(), byd.end(), [&](int64_t a, int64_t b) { return deg[a] < deg[b]; });
+    for (int64_t s0 : byd) {
+        if (seen[s0]) continue;
+        size_t head = order.size();
+        order.push_back(s0);
+        seen[s0] = 1;
+        while (head < order.size()) {
+            int64_t i = order[head++];
+            int64_t nb[4];
+            int cnt = 0;
+            for (int k = 0; k < 4; ++k) {
+                int32_t st = mv.cell_stiffness[cidx(n, i, k)];
+                if (st >= 1 && !seen[st - 1]) { nb[cnt++] = st - 1; seen[st - 1] = 1; }
+            }
+            std::sort(nb, nb + cnt, [&](int64_t a, int64_t b) { return deg[a] < deg[b]; });
+            for (int q = 0; q < cnt; ++q) order.push_back(nb[q]);
+        }
+    }
+    perm.assign(order.rbegin(), order.rend());
+}
+
+int validate_mesh(int c, const gd2d_mesh_view &mv, const gd2d_params &p) {
+    const int64_t n = mv.n_cells, nn = mv.n_nodes;
+    if (n <= 0 || nn <= 0) return fail(nullptr, GD2D_ERR_MESH, "case %d: empty mesh", c);
+    if (n >= (1LL << 30) || nn >= (1LL << 30)) return fail(nullptr, GD2D_ERR_MESH, "case %d: mesh too large", c);
+    if (!mv.mesh_connectivity || !mv.cell_stiffness || !mv.cell_edges_Nx || !mv.cell_edges_Ny ||
+        !mv.cell_edges_length || !mv.cell_areas || !mv.HX || !mv.cell_clusters || !mv.node2cellL2up ||
+        !mv.node2cellL2down || !mv.cells2nodes || !mv.cell_mid_points || !mv.x_nodes || !mv.y_nodes)
+        return fail(nullptr, GD2D_ERR_ARG, "case %d: a mesh array pointer is NULL", c);
+    if (mv.n_neib_cells < 1 || mv.n_neib_cells > 64)
+        return fail(nullptr, GD2D_ERR_MESH, "case %d: n_neib_cells=%d out of range", c, mv.n_neib_cells);
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t typ = mv.mesh_connectivity[cidx(n, i, 1)];
+        int32_t nf = mv.mesh_connectivity[cidx(n, i, 2)];
+        if (!((nf == 3 && typ == 3) || (nf == 4 && typ == 2)))
+            return fail(nullptr, GD2D_ERR_MESH, "case %d: cell %lld has type %d with %d nodes", c, (long long)i + 1,
+                        typ, nf);
+        if (!(mv.cell_areas[i] > 0.0))
+            return fail(nullptr, GD2D_ERR_MESH, "case %d: cell %lld has non-positive area", c, (long long)i + 1);
+        for (int k = 0; k < nf; ++k) {
+            int32_t st = mv.cell_stiffness[cidx(n, i, k)];
+            if (st > n || st == 0)
+                return fail(nullptr, GD2D_ERR_MESH, "case %d: cell %lld face %d neighbour %d out of range", c,
+                            (long long)i + 1, k + 1, st);
+            if (st < 0) {
+                bool found = false;
+                for (int b = 0; b < p.n_bc; ++b) found |= (p.bc[b].tag == st);
+                if (!found)
+                    return fail(nullptr, GD2D_ERR_MESH, "case %d: boundary tag %d has no entry in params.bc", c, st);
+            } else {
+                int idx = 2 * k;
+                int cntn = (nf == 4) ? 2 : 1;
+                for (int q = 0; q < cntn; ++q) {
+                    int32_t d = mv.node2cellL2down[cidx(n, i, idx + q)], u = mv.node2cellL2up[cidx(n, i, idx + q)];
+                    if (d < 1 || d > nn || u < 1 || u > nn)
+                        return fail(nullptr, GD2D_ERR_MESH, "case %d: cell %lld face %d: up/down node out of range", c,
+                                    (long long)i + 1, k + 1);
+                }
+            }
+            for (int q = 0; q < 2; ++q) {
+                int32_t e = mv.cells2nodes[cidx(n, i, 2 * k + q)];
+                if (e < 1 || e > nn)
+                    return fail(nullptr, GD2D_ERR_MESH, "case %d: cell %lld cells2nodes out of range", c,
+                                (long long)i + 1);
+            }
+        }
+    }
+    for (int64_t J = 0; J < nn; ++J)
+        for (int j = 0; j < mv.n_neib_cells; ++j) {
+            int32_t cc = mv.cell_clusters[cidx(nn, J, j)];
+            if (cc < 0 || cc > n)
+                return fail(nullptr, GD2D_ERR_MESH, "case %d: node %lld cluster entry %d out of range", c,
+                            (long long)J + 1, cc);
+        }
+    return GD2D_OK;
+}
+
+DevCase make_devcase(const gd2d_params &p, double maxEdge) {
+    DevCase d{};
+    d.gamma = p.Gamma;
+    d.R = p.RGAS;
+    d.CFL = p.CFL;
+    d.dt_fixed = p.dt;
+    d.beta = p.beta;
+    d.ksi = p.ksi;
+    d.venkat_K = p.venkat_K;
+    d.mu_ref = p.mu_ref;
+    d.suth_ref = 1.4792e-6 * std::sqrt(p.T_ref) / (1.0 + 116.0 / p.T_ref);
+    d.gamma_over_Pr = p.Gamma / p.Pr;
+    d.maxEdge = maxEdge;
+    d.tgv_U0 = p.tgv_U0;
+    d.tgv_P0 = p.tgv_P0;
+    d.tgv_L = p.tgv_L;
+    d.tgv_mu = p.tgv_mu;
+    for (int b = 0; b < kMaxBC; ++b) {
+        d.bc_kind[b] = b < p.n_bc ? p.bc[b].kind : BC_OUTFLOW;
+        d.bc_rho[b] = p.bc[b].rho;
+        d.bc_u[b] = p.bc[b].u;
+        d.bc_v[b] = p.bc[b].v;
+        d.bc_p[b] = p.bc[b].p;
+        d.bc_Tw[b] = p.bc[b].Tw;
+    }
+    d.dt_mode = p.dt_mode;
+    d.visc_model = p.viscosity;
+    d.art_visc = p.art_viscosity;
+    d.limiter = p.limiter;
+    return d;
+}
+
+template <class T>
+cudaError_t upload(T *dst, const std::vector<T> &src) {
+    if (src.empty()) return cudaSuccess;
+    return cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gd2d_abi_version(void) { return GD2D_ABI_VERSION; }
+
+const char *gd2d_last_error(const gd2d_handle *h) { return h ? h->err.c_str() : g_setup_error.c_str(); }
+
+int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes, const gd2d_params *params,
+               const gd2d_launch *launch) {
+    if (!out) return fail(nullptr, GD2D_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (n_cases < 1 || !meshes || !params) return fail(nullptr, GD2D_ERR_ARG, "need n_cases >= 1, meshes, params");
+    for (int c = 0; c < n_cases; ++c) {
+        const gd2d_params &p = params[c];
+        if (p.n_bc < 0 || p.n_bc > GD2D_MAX_BC) return fail(nullptr, GD2D_ERR_ARG, "case %d: n_bc out of range", c);
+        if (p.flux != params[0].flux || p.viscosity != params[0].viscosity ||
+            (p.viscosity != GD2D_VISC_NONE) != (params[0].viscosity != GD2D_VISC_NONE))
+            return fail(nullptr, GD2D_ERR_ARG, "flux and viscosity model must agree across the cases of a handle");
+        if (p.flux < 1 || p.flux > 3) return fail(nullptr, GD2D_ERR_ARG, "case %d: unknown flux %d", c, p.flux);
+        if (p.limiter < 0 || p.limiter > 4) return fail(nullptr, GD2D_ERR_ARG, "case %d: unknown limiter", c);
+        if (p.viscosity < 0 || p.viscosity > 3) return fail(nullptr, GD2D_ERR_ARG, "case %d: unknown viscosity", c);
+        if (p.dt_mode < 0 || p.dt_mode > 2) return fail(nullptr, GD2D_ERR_ARG, "case %d: unknown dt_mode", c);
+        if (!(p.Gamma > 1.0) || !(p.RGAS > 0.0)) return fail(nullptr, GD2D_ERR_ARG, "case %d: bad thermo", c);
+        if (p.dt_mode == GD2D_DT_FIXED && !(p.dt > 0.0)) return fail(nullptr, GD2D_ERR_ARG, "case %d: dt <= 0", c);
+        if (p.dt_mode != GD2D_DT_FIXED && !(p.CFL > 0.0)) return fail(nullptr, GD2D_ERR_ARG, "case %d: CFL <= 0", c);
+        if (p.viscosity == GD2D_VISC_SUTHERLAND && !(p.T_ref > 0.0 && p.Pr > 0.0))
+            return fail(nullptr, GD2D_ERR_ARG, "case %d: Sutherland needs T_ref > 0 and Pr > 0", c);
+        if (p.viscosity == GD2D_VISC_CONSTANT && !(p.Pr > 0.0))
+            return fail(nullptr, GD2D_ERR_ARG, "case %d: needs Pr > 0", c);
+        for (int b = 0; b < p.n_bc; ++b) {
+            if (p.bc[b].tag >= 0) return fail(nullptr, GD2D_ERR_ARG, "case %d: bc tags must be negative", c);
+            if (p.bc[b].kind < 1 || p.bc[b].kind > 5) return fail(nullptr, GD2D_ERR_ARG, "case %d: bad bc kind", c);
+            if (p.bc[b].kind == GD2D_BC_NOSLIP_ISOTHERMAL && !(p.bc[b].Tw > 0.0))
+                return fail(nullptr, GD2D_ERR_ARG, "case %d: isothermal wall needs Tw > 0", c);
+        }
+        int rc = validate_mesh(c, meshes[c], p);
+        if (rc != GD2D_OK) return rc;
+    }
+
+    gd2d_handle *h = new gd2d_handle();
+    h->ncases = n_cases;
+    if (launch) h->launch = *launch;
+    if (h->launch.precision != GD2D_PREC_F64) {
+        delete h;
+        return fail(nullptr, GD2D_ERR_ARG, "precision %d not available in this build", launch->precision);
+    }
+    int block = h->launch.block ? h->launch.block : 256;
+    if (block != 128 && block != 256) {
+        delete h;
+        return fail(nullptr, GD2D_ERR_ARG, "block must be 128 or 256");
+    }
+    h->lc.block = block;
+    h->lc.node_block = h->launch.node_block ? h->launch.node_block : 256;
+    h->lc.persistent = h->launch.persistent;
+    h->graph_steps = h->launch.graph_steps > 0 ? h->launch.graph_steps : 32;
+    h->flux = params[0].flux;
+    h->visc = params[0].viscosity != GD2D_VISC_NONE;
+    cudaGetDevice(&h->device);
+    if (h->launch.stream) {
+        h->stream = (cudaStream_t)h->launch.stream;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete h;
+            return fail(nullptr, GD2D_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        }
+        h->own_stream = true;
+    }
+
+    // ------------------------------------------------------- ordering
+    h->cases.resize(n_cases);
+    int64_t Nc = 0, Nn = 0;
+    int W = 1;
+    bool unit = true;
+    for (int c = 0; c < n_cases; ++c) {
+        const gd2d_mesh_view &mv = meshes[c];
+        HostCase &hc = h->cases[c];
+        hc.nc = mv.n_cells;
+        hc.nn = mv.n_nodes;
+        hc.params = params[c];
+        hc.start_time = params[c].start_time;
+        hc.nc_pad = (hc.nc + kCellPad - 1) / kCellPad * kCellPad;
+        hc.cell_off = Nc;
+        hc.node_off = Nn;
+        Nc += hc.nc_pad;
+        Nn += (hc.nn + 3) / 4 * 4;
+        for (int b = 0; b < params[c].n_bc; ++b) h->tgv |= params[c].bc[b].kind == GD2D_BC_TGV_ANALYTIC;
+        for (int64_t i = 0; i < hc.nc; ++i) h->quads |= mv.mesh_connectivity[cidx(hc.nc, i, 2)] == 4;
+        const int order = h->launch.order;
+        if (order == GD2D_ORDER_HILBERT) {
+            std::vector<double> xs(hc.nc), ys(hc.nc);
+            for (int64_t i = 0; i < hc.nc; ++i) {
+                xs[i] = mv.cell_mid_points[cidx(hc.nc, i, 0)];
+                ys[i] = mv.cell_mid_points[cidx(hc.nc, i, 1)];
+            }
+            hilbert_order(xs, ys, hc.cell_perm);
+            std::vector<double> nx(mv.x_nodes, mv.x_nodes + hc.nn), ny(mv.y_nodes, mv.y_nodes + hc.nn);
+            hilbert_order(nx, ny, hc.node_perm);
+        } else if (order == GD2D_ORDER_RCM) {
+            rcm_order(mv, hc.cell_perm);
+            hc.node_perm.resize(hc.nn);
+            std::iota(hc.node_perm.begin(), hc.node_perm.end(), 0);
+        } else {
+            hc.cell_perm.resize(hc.nc);
+            std::iota(hc.cell_perm.begin(), hc.cell_perm.end(), 0);
+            hc.node_perm.resize(hc.nn);
+            std::iota(hc.node_perm.begin(), hc.node_perm.end(), 0);
+        }
+        if (order == GD2D_ORDER_RCM) {
+            // nodes in order of first use by the reordered cells
+            std::vector<char> seen(hc.nn, 0);
+            std::vector<int64_t> np;
+            np.reserve(hc.nn);
+            for (int64_t j = 0; j < hc.nc; ++j) {
+                int64_t i = hc.cell_perm[j];
+                int nf = mv.mesh_connectivity[cidx(hc.nc, i, 2)];
+                for (int q = 0; q < nf; ++q) {
+                    int32_t v = mv.mesh_connectivity[cidx(hc.nc, i, 3 + q)] - 1;
+                    if (v >= 0 && v < hc.nn && !seen[v]) { seen[v] = 1; np.push_back(v); }
+                }
+            }
+            for (int64_t v = 0; v < hc.nn; ++v) if (!seen[v]) np.push_back(v);
+            hc.node_perm.swap(np);
+        }
+        hc.cell_inv.assign(hc.nc, 0);
+        for (int64_t j = 0; j < hc.nc; ++j) hc.cell_inv[hc.cell_perm[j]] = j;
+        hc.node_inv.assign(hc.nn, 0);
+        for (int64_t j = 0; j < hc.nn; ++j) hc.node_inv[hc.node_perm[j]] = j;
+        for (int64_t J = 0; J < hc.nn; ++J) {
+            int cnt = 0;
+            for (int j = 0; j < mv.n_neib_cells; ++j) {
+                int32_t cc = mv.cell_clusters[cidx(hc.nn, J, j)];
+                if (cc != 0) {
+                    ++cnt;
+                    if (mv.node_stencils[cidx(hc.nn, J, j)] != 1.0) unit = false;
+                }
+            }
+            W = std::max(W, cnt);
+        }
+    }
+    const int nfmax = h->quads ? 4 : 3;
+    const int64_t ntiles = Nc / block;
+
+    // ------------------------------------------------------- packing
+    std::vector<int4> nbr(Nc), dn(Nc), up(Nc), dn2, up2;
+    std::vector<int2> c2n((size_t)nfmax * Nc, make_int2(0, 0));
+    std::vector<double> gnx((size_t)nfmax * Nc, 0.0), gny((size_t)nfmax * Nc, 0.0), glen((size_t)nfmax * Nc, 0.0);
+    std::vector<double> rarea(Nc, 0.0), area(Nc, 0.0), hx(Nc, 0.0), charlen(Nc, 0.0);
+    std::vector<double2> mid;
+    std::vector<double> xnode, ynode;
+    std::vector<int32_t> cl((size_t)W * Nn, -1);
+    std::vector<double> wt;
+    if (!unit) wt.assign((size_t)W * Nn, 0.0);
+    if (h->quads) { dn2.assign(Nc, make_int4(0, 0, 0, 0)); up2.assign(Nc, make_int4(0, 0, 0, 0)); }
+    if (h->tgv) { mid.assign(Nc, make_double2(0.0, 0.0)); xnode.assign(Nn, 0.0); ynode.assign(Nn, 0.0); }
+    for (int64_t g = 0; g < Nc; ++g) nbr[g] = make_int4(kAbsent, kAbsent, kAbsent, kAbsent);
+    for (int64_t g = 0; g < Nc; ++g) { dn[g] = make_int4(0, 0, 0, 0); up[g] = make_int4(0, 0, 0, 0); }
+    std::vector<int32_t> tile_case(ntiles, 0);
+    h->hcases.resize(n_cases);
+    for (int c = 0; c < n_cases; ++c) {
+        const gd2d_mesh_view &mv = meshes[c];
+        HostCase &hc = h->cases[c];
+        const int64_t n = hc.nc, nn = hc.nn;
+        double maxEdge = mv.HX[0];
+        for (int64_t i = 1; i < n; ++i) maxEdge = std::max(maxEdge, mv.HX[i]);
+        auto node_g = [&](int32_t id1) -> int32_t {  // 1-based reference id -> global new id
+            if (id1 < 1) return 0;
+            return (int32_t)(hc.node_off + hc.node_inv[id1 - 1]);
+        };
+        for (int64_t j = 0; j < n; ++j) {
+            const int64_t i = hc.cell_perm[j];
+            const int64_t g = hc.cell_off + j;
+            const int nf = mv.mesh_connectivity[cidx(n, i, 2)];
+            int nb[4] = {kAbsent, kAbsent, kAbsent, kAbsent};
+            int d1[4] = {0, 0, 0, 0}, u1[4] = {0, 0, 0, 0}, d2[4] = {0, 0, 0, 0}, u2[4] = {0, 0, 0, 0};
+            double per = 0.0;
+            for (int k = 0; k < nf; ++k) {
+                int32_t st = mv.cell_stiffness[cidx(n, i, k)];
+                if (st >= 1) {
+                    nb[k] = (int32_t)(hc.cell_off + hc.cell_inv[st - 1]);
+                    d1[k] = node_g(mv.node2cellL2down[cidx(n, i, 2 * k)]);
+                    u1[k] = node_g(mv.node2cellL2up[cidx(n, i, 2 * k)]);
+                    if (nf == 4) {
+                        d2[k] = node_g(mv.node2cellL2down[cidx(n, i, 2 * k + 1)]);
+                        u2[k] = node_g(mv.node2cellL2up[cidx(n, i, 2 * k + 1)]);
+                    }
+                } else {
+                    int slot = 0;
+                    for (int b = 0; b < hc.params.n_bc; ++b) if (hc.params.bc[b].tag == st) { slot = b; break; }
+                    nb[k] = -(slot + 1);
+                }
+                const size_t o = (size_t)k * Nc + g;
+                gnx[o] = mv.cell_edges_Nx[cidx(n, i, k)];
+                gny[o] = mv.cell_edges_Ny[cidx(n, i, k)];
+                glen[o] = mv.cell_edges_length[cidx(n, i, k)];
+                c2n[o] = make_int2(node_g(mv.cells2nodes[cidx(n, i, 2 * k)]), node_g(mv.cells2nodes[cidx(n, i, 2 * k + 1)]));
+                per += mv.cell_edges_length[cidx(n, i, k)];
+            }
+            nbr[g] = make_int4(nb[0], nb[1], nb[2], nb[3]);
+            dn[g] = make_int4(d1[0], d1[1], d1[2], d1[3]);
+            up[g] = make_int4(u1[0], u1[1], u1[2], u1[3]);
+            if (h->quads) { dn2[g] = make_int4(d2[0], d2[1], d2[2], d2[3]); up2[g] = make_int4(u2[0], u2[1], u2[2], u2[3]); }
+            const double A = mv.cell_areas[i];
+            area[g] = A;
+            rarea[g] = 1.0 / A;
+            hx[g] = mv.HX[i];
+            charlen[g] = 2.0 * A / per;
+            if (h->tgv) mid[g] = make_double2(mv.cell_mid_points[cidx(n, i, 0)], mv.cell_mid_points[cidx(n, i, 1)]);
+        }
+        for (int64_t j = 0; j < nn; ++j) {
+            const int64_t J = hc.node_perm[j];
+            const int64_t gn = hc.node_off + j;
+            int slot = 0;
+            for (int q = 0; q < mv.n_neib_cells; ++q) {
+                int32_t cc = mv.cell_clusters[cidx(nn, J, q)];
+                if (cc != 0) {
+                    cl[(size_t)slot * Nn + gn] = (int32_t)(hc.cell_off + hc.cell_inv[cc - 1]);
+                    if (!unit) wt[(size_t)slot * Nn + gn] = mv.node_stencils[cidx(nn, J, q)];
+                    ++slot;
+                }
+            }
+            if (h->tgv) { xnode[gn] = mv.x_nodes[J]; ynode[gn] = mv.y_nodes[J]; }
+        }
+        DevCase d = make_devcase(hc.params, maxEdge);
+        d.cell_begin = hc.cell_off;
+        d.cell_end = hc.cell_off + hc.nc_pad;
+        d.tile_begin = hc.cell_off / block;
+        d.tile_end = (hc.cell_off + hc.nc_pad) / block;
+        for (int64_t t = d.tile_begin; t < d.tile_end; ++t) tile_case[t] = c;
+        h->hcases[c] = d;
+    }
+    h->tile_case_h = tile_case;
+
+    // ------------------------------------------------------- device
+    cudaSetDevice(h->device);
+    DevMesh &m = h->m;
+    DevState &s = h->s;
+    m.Nc = Nc; m.Nn = Nn; m.ncases = n_cases; m.nfmax = nfmax; m.cluster_w = W; m.unit_weights = unit ? 1 : 0;
+    m.ntiles = ntiles;
+    int4 *d_nbr, *d_dn, *d_up, *d_dn2 = nullptr, *d_up2 = nullptr;
+    int2 *d_c2n;
+    double *d_nx, *d_ny, *d_len, *d_rarea, *d_area, *d_hx, *d_charlen, *d_xn = nullptr, *d_yn = nullptr, *d_wt = nullptr;
+    double2 *d_mid = nullptr;
+    int32_t *d_cl, *d_tc;
+    DevCase *d_cases;
+    auto bail = [&](int rc) { h->buf.free_all(); if (h->own_stream) cudaStreamDestroy(h->stream); g_setup_error = h->err; delete h; return rc; };
+#define ALLOC(ptr, n)                                                                              \
+    do {                                                                                           \
+        cudaError_t e__ = h->buf.alloc(&(ptr), (size_t)(n));                                       \
+        if (e__ != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaMalloc %s: %s", #ptr, cudaGetErrorString(e__))); \
+    } while (0)
+#define UPLOAD(ptr, vec)                                                                           \
+    do {                                                                                           \
+        cudaError_t e__ = upload((ptr), (vec));                                                    \
+        if (e__ != cudaSuccess) return bail(fail(h, GD2D_ERR_CUDA, "upload %s: %s", #ptr, cudaGetErrorString(e__))); \
+    } while (0)
+    ALLOC(d_nbr, Nc); UPLOAD(d_nbr, nbr);
+    ALLOC(d_dn, Nc); UPLOAD(d_dn, dn);
+    ALLOC(d_up, Nc); UPLOAD(d_up, up);
+    if (h->quads) { ALLOC(d_dn2, Nc); UPLOAD(d_dn2, dn2); ALLOC(d_up2, Nc); UPLOAD(d_up2, up2); }
+    ALLOC(d_c2n, (size_t)nfmax * Nc); UPLOAD(d_c2n, c2n);
+    ALLOC(d_nx, (size_t)nfmax * Nc); UPLOAD(d_nx, gnx);
+    ALLOC(d_ny, (size_t)nfmax * Nc); UPLOAD(d_ny, gny);
+    ALLOC(d_len, (size_t)nfmax * Nc); UPLOAD(d_len, glen);
+    ALLOC(d_rarea, Nc); UPLOAD(d_rarea, rarea);
+    ALLOC(d_area, Nc); UPLOAD(d_area, area);
+    ALLOC(d_hx, Nc); UPLOAD(d_hx, hx);
+    ALLOC(d_charlen, Nc); UPLOAD(d_charlen, charlen);
+    if (h->tgv) {
+        ALLOC(d_mid, Nc); UPLOAD(d_mid, mid);
+        ALLOC(d_xn, Nn); UPLOAD(d_xn, xnode);
+        ALLOC(d_yn, Nn); UPLOAD(d_yn, ynode);
+    }
+    ALLOC(d_cl, (size_t)W * Nn); UPLOAD(d_cl, cl);
+    if (!unit) { ALLOC(d_wt, (size_t)W * Nn); UPLOAD(d_wt, wt); }
+    ALLOC(d_tc, ntiles); UPLOAD(d_tc, tile_case);
+    ALLOC(d_cases, n_cases); UPLOAD(d_cases, h->hcases);
+    m.nbr = d_nbr; m.dn = d_dn; m.up = d_up; m.dn2 = d_dn2; m.up2 = d_up2; m.c2n = d_c2n;
+    m.nx = d_nx; m.ny = d_ny; m.len = d_len; m.rarea = d_rarea; m.area = d_area; m.hx = d_hx; m.charlen = d_charlen;
+    m.mid = d_mid; m.xnode = d_xn; m.ynode = d_yn; m.cl = d_cl; m.wt = d_wt; m.tile_case = d_tc; m.cases = d_cases;
+
+    s.ring_len = 1024;
+    ALLOC(s.U, Nc);
+    ALLOC(s.prim, 2 * Nc);
+    ALLOC(s.nodeP, Nn);
+    if (h->visc) { ALLOC(s.nodeC, Nn); ALLOC(s.g1, Nc); ALLOC(s.nodeG, Nn); }
+    ALLOC(s.part, (size_t)ntiles * kPartials);
+    ALLOC(s.cstate, n_cases);
+    ALLOC(s.ring, (size_t)s.ring_len * n_cases);
+    ALLOC(s.parity, 1);
+    ALLOC(s.node_done, 1);
+#undef ALLOC
+#undef UPLOAD
+    {
+        int dev_sms = 148;
+        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
+        int per_sm = 0;
+        h->lc.grid = dev_sms * 8;
+        (void)per_sm;
+    }
+    h->history.assign(n_cases, {});
+    cudaEventCreate(&h->ev_total[0]);
+    cudaEventCreate(&h->ev_total[1]);
+    *out = h;
+    return GD2D_OK;
+}
+
+static int ensure_case(gd2d_handle *h, int32_t icase) {
+    if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");
+    if (icase < 0 || icase >= h->ncases) return fail(h, GD2D_ERR_ARG, "case index %d out of range", icase);
+    return GD2D_OK;
+}
+
+static int drop_graph(gd2d_handle *h) {
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+    h->ev.clear();
+    return GD2D_OK;
+}
+
+// Upload cell primitives (reference order) of one case and rebuild U, the
+// node fields and the first dt of that case.
+static int init_case_from_prims(gd2d_handle *h, int32_t icase, const std::vector<double4> &prims_new_order,
+                                double t0, bool nodes_from_cells) {
+    HostCase &hc = h->cases[icase];
+    cudaSetDevice(h->device);
+    int par = 0;
+    CUDA_TRY(h, cudaMemcpy(&par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(h, cudaMemcpy(h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, prims_new_order.data(),
+                           sizeof(double4) * hc.nc, cudaMemcpyHostToDevice));
+    CaseState cs{};
+    cs.t = t0;
+    CUDA_TRY(h, cudaMemcpy(h->s.cstate + icase, &cs, sizeof cs, cudaMemcpyHostToDevice));
+    // Per-case init restricted to this case's tiles and nodes.
+    const DevCase &d = h->hcases[icase];
+    CUDA_TRY(h, launch_init_state_f64(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
+    CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off, hc.node_off + hc.nn,
+                                    h->lc, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    hc.state_set = true;
+    h->history[icase].clear();
+    bool all = true;
+    for (auto &c : h->cases) all &= c.state_set;
+    h->state_ready = all;
+    return GD2D_OK;
+}
+
+int gd2d_set_state(gd2d_handle *h, int32_t icase, const double *density, const double *ux, const double *uy,
+                   const double *pressure) {
+    int rc = ensure_case(h, icase);
+    if (rc) return rc;
+    if (!density || !ux || !uy || !pressure) return fail(h, GD2D_ERR_ARG, "NULL field pointer");
+    HostCase &hc = h->cases[icase];
+    std::vector<double4> pr(hc.nc);
+    for (int64_t j = 0; j < hc.nc; ++j) {
+        int64_t i = hc.cell_perm[j];
+        pr[j] = make_double4(density[i], ux[i], uy[i], pressure[i]);
+    }
+    return init_case_from_prims(h, icase, pr, hc.start_time, hc.params.init_nodes != 0);
+}
+
+int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, double flow_time, int32_t rebuild_nodes) {
+    int rc = ensure_case(h, icase);
+    if (rc) return rc;
+    if (!ucons) return fail(h, GD2D_ERR_ARG, "NULL ucons");
+    HostCase &hc = h->cases[icase];
+    const double G = hc.params.Gamma;
+    std::vector<double4> pr(hc.nc);
+    for (int64_t j = 0; j < hc.nc; ++j) {
+        int64_t i = hc.cell_perm[j];
+        double U1 = ucons[cidx(hc.nc, i, 0)], U2 = ucons[cidx(hc.nc, i, 1)], U3 = ucons[cidx(hc.nc, i, 2)],
+               U4 = ucons[cidx(hc.nc, i, 3)];
+        pr[j] = make_double4(U1, U2 / U1, U3 / U1, (G - 1.0) * (U4 - 0.5 * (U2 * U2 + U3 * U3) / U1));
+    }
+    return init_case_from_prims(h, icase, pr, flow_time, rebuild_nodes != 0);
+}
+
+static int capture_graph(gd2d_handle *h, int steps, bool timing) {
+    drop_graph(h);
+    if (timing) {
+        h->ev.resize(2 * steps);
+        for (auto &e : h->ev) CUDA_TRY(h, cudaEventCreate(&e));
+    }
+    cudaGraph_t g;
+    CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < steps; ++k) {
+        if (h->visc) launch_visc_grad_f64(h->m, h->s, h->lc, h->stream);
+        if (timing) cudaEventRecord(h->ev[2 * k], h->stream);
+        launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream);
+        if (timing) cudaEventRecord(h->ev[2 * k + 1], h->stream);
+        launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream);
+    }
+    CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    return GD2D_OK;
+}
+
+int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
+    if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");
+    if (nsteps < 0) return fail(h, GD2D_ERR_ARG, "nsteps < 0");
+    if (!h->state_ready) return fail(h, GD2D_ERR_STATE, "gd2d_set_state must be called for every case first");
+    cudaSetDevice(h->device);
+    const int G = h->graph_steps;
+    const bool timing = true;
+    int64_t launches = 0;
+    double total_ms = 0.0, cell_ms = 0.0;
+    int cell_samples = 0;
+    int32_t done = 0;
+    std::vector<int64_t> step0(h->ncases);
+    while (done < nsteps) {
+        const int32_t chunk = std::min<int32_t>(nsteps - done, h->s.ring_len);
+        std::vector<CaseState> before(h->ncases);
+        CUDA_TRY(h, cudaMemcpy(before.data(), h->s.cstate, sizeof(CaseState) * h->ncases, cudaMemcpyDeviceToHost));
+        CUDA_TRY(h, cudaEventRecord(h->ev_total[0], h->stream));
+        int32_t k = 0;
+        bool used_graph = false;
+        if (G > 1) {
+            while (chunk - k >= G) {
+                if (!h->graph) {
+                    int rc = capture_graph(h, G, timing);
+                    if (rc) return rc;
+                }
+                CUDA_TRY(h, cudaGraphLaunch(h->graph, h->stream));
+                used_graph = true;
+                k += G;
+                launches += (int64_t)G * (h->visc ? 4 : 2);
+            }
+        }
+        for (; k < chunk; ++k) {
+            if (h->visc) CUDA_TRY(h, launch_visc_grad_f64(h->m, h->s, h->lc, h->stream));
+            CUDA_TRY(h, launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream));
+            CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream));
+            launches += h->visc ? 4 : 2;
+        }
+        CUDA_TRY(h, cudaEventRecord(h->ev_total[1], h->stream));
+        CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev_total[0], h->ev_total[1]);
+        total_ms += ms;
+        if (used_graph && timing && !h->ev.empty()) {
+            for (int q = 0; q < G; ++q) {
+                float c = 0.f;
+                if (cudaEventElapsedTime(&c, h->ev[2 * q], h->ev[2 * q + 1]) == cudaSuccess) {
+                    cell_ms += c;
+                    ++cell_samples;
+                }
+            }
+        }
+        // history
+        std::vector<DevStats> ring((size_t)h->s.ring_len * h->ncases);
+        CUDA_TRY(h, cudaMemcpy(ring.data(), h->s.ring, sizeof(DevStats) * ring.size(), cudaMemcpyDeviceToHost));
+        bool bad = false;
+        for (int c = 0; c < h->ncases; ++c) {
+            for (int32_t q = 0; q < chunk; ++q) {
+                int64_t stp = before[c].step + q;
+                const DevStats &ds = ring[(size_t)(stp % h->s.ring_len) * h->ncases + c];
+                gd2d_stats st;
+                static_assert(sizeof(gd2d_stats) == sizeof(DevStats), "stats layout");
+                std::memcpy(&st, &ds, sizeof st);
+                h->history[c].push_back(st);
+                bad |= st.nonfinite != 0;
+            }
+            if (stats_out) stats_out[c] = h->history[c].back();
+        }
+        done += chunk;
+        if (bad) return fail(h, GD2D_ERR_NONFINITE, "non-finite or non-positive state after step %lld",
+                             (long long)(before[0].step + chunk));
+    }
+    h->last_total_ms = total_ms;
+    h->last_cell_ms = cell_samples ? cell_ms / cell_samples : 0.0;
+    h->last_launches = launches;
+    return GD2D_OK;
+}
+
+int gd2d_get_history(gd2d_handle *h, int32_t icase, gd2d_stats *out, int32_t capacity) {
+    int rc = ensure_case(h, icase);
+    if (rc) return rc;
+    const auto &v = h->history[icase];
+    int32_t n = (int32_t)std::min<size_t>(v.size(), (size_t)std::max(capacity, 0));
+    if (out) std::memcpy(out, v.data() + (v.size() - n), sizeof(gd2d_stats) * n);
+    return n;
+}
+
+int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, double *node_prims) {
+    int rc = ensure_case(h, icase);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    HostCase &hc = h->cases[icase];
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    int par = 0;
+    CUDA_TRY(h, cudaMemcpy(&par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<double4> tmp(std::max(hc.nc, hc.nn));
+    if (ucons) {
+        CUDA_TRY(h, cudaMemcpy(tmp.data(), h->s.U + hc.cell_off, sizeof(double4) * hc.nc, cudaMemcpyDeviceToHost));
+        for (int64_t j = 0; j < hc.nc; ++j) {
+            int64_t i = hc.cell_perm[j];
+            ucons[cidx(hc.nc, i, 0)] = tmp[j].x; ucons[cidx(hc.nc, i, 1)] = tmp[j].y;
+            ucons[cidx(hc.nc, i, 2)] = tmp[j].z; ucons[cidx(hc.nc, i, 3)] = tmp[j].w;
+        }
+    }
+    if (prims) {
+        CUDA_TRY(h, cudaMemcpy(tmp.data(), h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, sizeof(double4) * hc.nc,
+                               cudaMemcpyDeviceToHost));
+        for (int64_t j = 0; j < hc.nc; ++j) {
+            int64_t i = hc.cell_perm[j];
+            prims[cidx(hc.nc, i, 0)] = tmp[j].x; prims[cidx(hc.nc, i, 1)] = tmp[j].y;
+            prims[cidx(hc.nc, i, 2)] = tmp[j].z; prims[cidx(hc.nc, i, 3)] = tmp[j].w;
+        }
+    }
+    if (node_prims) {
+        CUDA_TRY(h, cudaMemcpy(tmp.data(), h->s.nodeP + hc.node_off, sizeof(double4) * hc.nn, cudaMemcpyDeviceToHost));
+        for (int64_t j = 0; j < hc.nn; ++j) {
+            int64_t J = hc.node_perm[j];
+            node_prims[cidx(hc.nn, J, 0)] = tmp[j].x; node_prims[cidx(hc.nn, J, 1)] = tmp[j].y;
+            node_prims[cidx(hc.nn, J, 2)] = tmp[j].z; node_prims[cidx(hc.nn, J, 3)] = tmp[j].w;
+        }
+    }
+    return GD2D_OK;
+}
+
+int gd2d_calc_one_stage(gd2d_handle *h, int32_t icase, double, double, double, double *, double *) {
+    int rc = ensure_case(h, icase);
+    if (rc) return rc;
+    return fail(h, GD2D_ERR_STATE, "gd2d_calc_one_stage: not built yet");
+}
+int gd2d_update_variables(gd2d_handle *h, int32_t icase, double *) {
+    int rc = ensure_case(h, icase);
+    if (rc) return rc;
+    return fail(h, GD2D_ERR_STATE, "gd2d_update_variables: not built yet");
+}
+int gd2d_cells_to_nodes(gd2d_handle *h) {
+    if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");
+    return fail(h, GD2D_ERR_STATE, "gd2d_cells_to_nodes: not built yet");
+}
+int gd2d_calc_diff_term(gd2d_handle *h, int32_t icase, double *) {
+    int rc = ensure_case(h, icase);
+    if (rc) return rc;
+    return fail(h, GD2D_ERR_STATE, "gd2d_calc_diff_term: not built yet");
+}
+int gd2d_autotune(gd2d_handle *h, int32_t, gd2d_launch *) {
+    if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");
+    return fail(h, GD2D_ERR_STATE, "gd2d_autotune: not built yet");
+}
+
+int gd2d_last_timing(gd2d_handle *h, double *total_ms, double *cell_kernel_ms, int64_t *launches) {
+    if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");
+    if (total_ms) *total_ms = h->last_total_ms;
+    if (cell_kernel_ms) *cell_kernel_ms = h->last_cell_ms;
+    if (launches) *launches = h->last_launches;
+    return GD2D_OK;
+}
+
+int gd2d_destroy(gd2d_handle *h) {
+    if (!h) return GD2D_OK;
+    cudaSetDevice(h->device);
+    cudaStreamSynchronize(h->stream);
+    drop_graph(h);
+    for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
+    h->buf.free_all();
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return GD2D_OK;
+}
+
+}  // extern "C"

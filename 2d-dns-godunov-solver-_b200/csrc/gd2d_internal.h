@@ -1,0 +1,129 @@
+// Internal device-side data structures of the godunov2d library.
+//
+// Layout in HBM (all cases of a handle concatenated; every case's cell range
+// padded to a multiple of kCellPad so that a tile of the cell kernel never
+// straddles two cases):
+//   per cell  : int4 nbr (neighbour cell or -(bc_slot+1), kAbsent for no face),
+//               int4 dn/up (down/up node per face; quads: dn2/up2 second node),
+//               int2 c2n[k] (edge node pair, viscous and TGV only),
+//               geometry planes nx[k], ny[k], len[k] (k < faces), rarea, area,
+//               hx, charlen, mid (x,y);
+//   state     : double4 U (rho, rho u, rho v, E) updated in place,
+//               prim[2] double4 (rho, u, v, p) double-buffered by step parity;
+//   per node  : double4 nodeP (weighted primitive average),
+//               double4 nodeC (unweighted mean of rho u, rho v, E) and
+//               NodeGrad nodeG (unweighted mean of the first gradients),
+//               ELL cluster lists cl[w][node] / wt[w][node].
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gd2d {
+
+constexpr int kCellPad = 1024;      // case cell ranges are multiples of this
+constexpr int kMaxBC = 8;
+constexpr int32_t kAbsent = INT32_MIN;
+constexpr int kPartials = 16;       // doubles per tile partial record
+constexpr int kMaxCluster = 8;
+
+enum FluxKind { FLUX_AUSM = 1, FLUX_ROE = 2, FLUX_AUSM_M2020 = 3 };
+enum LimKind { LIM_NONE = 0, LIM_MINMOD = 1, LIM_VENKAT = 2, LIM_VANLEER = 3, LIM_VANALBADA = 4 };
+enum BcKind { BC_INFLOW = 1, BC_OUTFLOW = 2, BC_SLIP = 3, BC_NOSLIP_ISOTHERMAL = 4, BC_TGV = 5 };
+enum ViscKind { VISC_NONE = 0, VISC_REFERENCE = 1, VISC_SUTHERLAND = 2, VISC_CONSTANT = 3 };
+enum DtMode { DT_FIXED = 0, DT_REFERENCE_TAU = 1, DT_LOCAL_CFL = 2 };
+
+// Partial record slots.
+enum PartSlot {
+    P_RES0 = 0, P_TOT0 = 4, P_EK = 8, P_VMAX = 9, P_RMIN = 10, P_RHOMIN = 11, P_RHOMAX = 12,
+    P_BAD = 13
+};
+
+// Per-case constants (read-only on the device).
+struct DevCase {
+    double gamma, R, CFL, dt_fixed, beta, ksi, venkat_K;
+    double mu_ref, suth_ref, gamma_over_Pr, maxEdge;
+    double tgv_U0, tgv_P0, tgv_L, tgv_mu;
+    double bc_rho[kMaxBC], bc_u[kMaxBC], bc_v[kMaxBC], bc_p[kMaxBC], bc_Tw[kMaxBC];
+    int32_t bc_kind[kMaxBC];
+    int32_t dt_mode, visc_model, art_visc, limiter;
+    int64_t cell_begin, cell_end;   // padded global cell range [begin, end)
+    int64_t tile_begin, tile_end;   // tiles of the cell kernel
+};
+
+// Per-case mutable step state (device).
+struct CaseState {
+    double t, dt, velmax, rmin;
+    int64_t step;
+    unsigned int tiles_done;
+    int32_t nonfinite;
+};
+
+// Mirrors gd2d_stats (include/godunov2d.h).
+struct DevStats {
+    double dt, flow_time, tau, velmax;
+    double residual[4];
+    double rho_min, rho_max;
+    double totals[4];
+    double kinetic_energy;
+    int64_t step;
+    int32_t nonfinite;
+    int32_t reserved0;
+};
+
+struct NodeGrad {  // unweighted node means of the first gradients
+    double2 ru, rv, re;  // (gradX, gradY) of rho u, rho v, E
+};
+
+struct DevMesh {
+    int64_t Nc, Nn;          // padded totals
+    int32_t ncases, nfmax;   // nfmax: 3 or 4
+    int32_t cluster_w;       // ELL width of the cluster lists
+    int32_t unit_weights;    // all node_stencils on live slots are 1.0
+    int64_t ntiles;
+    const int4 *nbr;
+    const int4 *dn, *up, *dn2, *up2;     // dn2/up2 only with quads
+    const int2 *c2n;                     // [nfmax][Nc] edge node pairs
+    const double *nx, *ny, *len;         // [nfmax][Nc]
+    const double *rarea, *area, *hx, *charlen;
+    const double2 *mid;                  // TGV only
+    const double *xnode, *ynode;         // TGV only
+    const int32_t *cl;                   // [cluster_w][Nn], -1 = empty
+    const double *wt;                    // [cluster_w][Nn] (NULL if unit weights)
+    const int32_t *tile_case;            // [ntiles]
+    const DevCase *cases;
+};
+
+struct DevState {
+    double4 *U;        // [Nc]
+    double4 *prim;     // [2][Nc]
+    double4 *nodeP;    // [Nn]
+    double4 *nodeC;    // [Nn] (viscous)
+    NodeGrad *g1;      // [Nc] (viscous) first gradients per cell
+    NodeGrad *nodeG;   // [Nn] (viscous)
+    double *part;      // [ntiles][kPartials]
+    CaseState *cstate; // [ncases]
+    DevStats *ring;    // [ring_len][ncases]
+    int32_t *parity;   // step parity (which prim buffer is current)
+    unsigned int *node_done;
+    int32_t ring_len;
+    int32_t pad_;
+};
+
+struct LaunchCfg {
+    int block;       // cell kernel threads per block (tile size)
+    int node_block;
+    int persistent;
+    int grid;        // persistent grid size
+};
+
+// Launchers implemented in kernels_f64.cu.
+cudaError_t launch_cell_step_f64(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
+                                 const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, bool flip_parity,
+                                bool zero_prims, int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,
+                                  cudaStream_t st);
+
+}  // namespace gd2d

@@ -1,0 +1,74 @@
+// FP64 instantiations of the step kernels.  This translation unit is built
+// with -fmad=false: like the reference's Julia Float64 code, no multiply-add
+// is contracted except the explicit fma() standing for the reference's
+// muladd, so results round exactly like the CPU restatement.
+#include "step_kernels.cuh"
+
+namespace gd2d {
+
+namespace {
+
+int grid_for(int64_t work, int block) {
+    int64_t g = (work + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 148LL * 64) g = 148 * 64;
+    return (int)g;
+}
+
+template <int FLUX, bool VISC, bool QUAD>
+cudaError_t cell_step(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
+    int grid = lc.persistent ? lc.grid : (int)m.ntiles;
+    k_cell_step<FLUX, VISC, QUAD><<<grid, lc.block, 0, st>>>(m, s);
+    return cudaGetLastError();
+}
+
+template <int FLUX>
+cudaError_t cell_step_flux(const DevMesh &m, const DevState &s, bool visc, bool quads, const LaunchCfg &lc,
+                           cudaStream_t st) {
+    if (visc) return quads ? cell_step<FLUX, true, true>(m, s, lc, st) : cell_step<FLUX, true, false>(m, s, lc, st);
+    return quads ? cell_step<FLUX, false, true>(m, s, lc, st) : cell_step<FLUX, false, false>(m, s, lc, st);
+}
+
+}  // namespace
+
+cudaError_t launch_cell_step_f64(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
+                                 const LaunchCfg &lc, cudaStream_t st) {
+    switch (flux) {
+    case FLUX_ROE: return cell_step_flux<FLUX_ROE>(m, s, visc, quads, lc, st);
+    case FLUX_AUSM_M2020: return cell_step_flux<FLUX_AUSM_M2020>(m, s, visc, quads, lc, st);
+    default: return cell_step_flux<FLUX_AUSM>(m, s, visc, quads, lc, st);
+    }
+}
+
+cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, bool flip_parity, bool zero_prims,
+                                int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st) {
+    const int b = lc.node_block;
+    const int grid = grid_for(n1 - n0, b);
+    const bool unit = m.unit_weights != 0;
+    if (visc) {
+        if (unit) k_node_avg<true, true><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+        else k_node_avg<true, false><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+    } else {
+        if (unit) k_node_avg<false, true><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+        else k_node_avg<false, false><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
+    const int b = lc.node_block;
+    if (m.nfmax == 4) k_grad1_cells<true><<<grid_for(m.Nc, b), b, 0, st>>>(m, s);
+    else k_grad1_cells<false><<<grid_for(m.Nc, b), b, 0, st>>>(m, s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_grad1_nodes<<<grid_for(m.Nn, b), b, 0, st>>>(m, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,
+                                  cudaStream_t st) {
+    k_init_state<<<(int)(t1 - t0), lc.block, 0, st>>>(m, s, t0, t1);
+    return cudaGetLastError();
+}
+
+}  // namespace gd2d

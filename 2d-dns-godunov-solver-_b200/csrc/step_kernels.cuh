@@ -1,0 +1,488 @@
+// Kernels of the explicit Godunov step (FP64 state and arithmetic).
+//
+// One step = [viscous: grad1 cell pass, grad1 node pass] -> fused cell
+// kernel -> node kernel.  The fused cell kernel does, per cell,
+// calcOneStageMUSCLcpuFast (calcOneStageMUSCLcpuFast.jl:3-107) followed by
+// updateVariablesSA (evaluate2d.jl:52-110) and the step's reductions; the
+// last tile of each case finalizes that case's statistics and next time step
+// (no device-wide barrier, no spin: a per-case ticket counter elects it).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "gd2d_internal.h"
+#include "physics.cuh"
+
+namespace gd2d {
+
+__device__ __forceinline__ int nbr_k(const int4 &v, int k) {
+    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+
+// ------------------------------------------------------- block reductions
+
+struct Part {
+    double res[4], tot[4], ek, vmax, rmin, rhomin, rhomax, bad;
+    __device__ void init() {
+        for (int v = 0; v < 4; ++v) { res[v] = 0.0; tot[v] = 0.0; }
+        ek = 0.0; vmax = 0.0; rmin = INFINITY; rhomin = INFINITY; rhomax = -INFINITY; bad = 0.0;
+    }
+    __device__ void combine(const Part &o) {
+        for (int v = 0; v < 4; ++v) { res[v] += o.res[v]; tot[v] += o.tot[v]; }
+        ek += o.ek;
+        vmax = fmax(vmax, o.vmax);
+        rmin = fmin(rmin, o.rmin);
+        rhomin = fmin(rhomin, o.rhomin);
+        rhomax = fmax(rhomax, o.rhomax);
+        bad = fmax(bad, o.bad);
+    }
+    __device__ void shfl_down(int off) {
+        Part o;
+        for (int v = 0; v < 4; ++v) {
+            o.res[v] = __shfl_down_sync(0xffffffffu, res[v], off);
+            o.tot[v] = __shfl_down_sync(0xffffffffu, tot[v], off);
+        }
+        o.ek = __shfl_down_sync(0xffffffffu, ek, off);
+        o.vmax = __shfl_down_sync(0xffffffffu, vmax, off);
+        o.rmin = __shfl_down_sync(0xffffffffu, rmin, off);
+        o.rhomin = __shfl_down_sync(0xffffffffu, rhomin, off);
+        o.rhomax = __shfl_down_sync(0xffffffffu, rhomax, off);
+        o.bad = __shfl_down_sync(0xffffffffu, bad, off);
+        combine(o);
+    }
+    __device__ void store(double *p) const {
+        for (int v = 0; v < 4; ++v) { p[P_RES0 + v] = res[v]; p[P_TOT0 + v] = tot[v]; }
+        p[P_EK] = ek; p[P_VMAX] = vmax; p[P_RMIN] = rmin; p[P_RHOMIN] = rhomin; p[P_RHOMAX] = rhomax;
+        p[P_BAD] = bad;
+    }
+    __device__ void load_cg(const double *p) {
+        for (int v = 0; v < 4; ++v) { res[v] = __ldcg(p + P_RES0 + v); tot[v] = __ldcg(p + P_TOT0 + v); }
+        ek = __ldcg(p + P_EK); vmax = __ldcg(p + P_VMAX); rmin = __ldcg(p + P_RMIN);
+        rhomin = __ldcg(p + P_RHOMIN); rhomax = __ldcg(p + P_RHOMAX); bad = __ldcg(p + P_BAD);
+    }
+};
+
+// Deterministic block reduction (fixed tree for a fixed blockDim); the
+// result is valid in thread 0.  `sh` holds blockDim/32 records.
+__device__ __forceinline__ void block_reduce(Part &p, Part *sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int off = 16; off > 0; off >>= 1) p.shfl_down(off);
+    if (lane == 0) sh[warp] = p;
+    __syncthreads();
+    if (warp == 0) {
+        if (lane < nw) p = sh[lane];
+        else p.init();
+        for (int off = 16; off > 0; off >>= 1) p.shfl_down(off);
+    }
+    __syncthreads();
+}
+
+// Per-case finalization by the block that completed the case's last tile:
+// reduce the tile records in a fixed order, publish the step statistics and
+// advance time (flowTime += dt, testInviscidFluxesGPUx32.jl:401) and the
+// next dt (tau at :322-324, or the local-CFL extension).
+__device__ void finalize_case(const DevMesh &m, const DevState &s, int c, Part *sh, bool is_init) {
+    const DevCase &P = m.cases[c];
+    Part acc;
+    acc.init();
+    for (int64_t t = P.tile_begin + threadIdx.x; t < P.tile_end; t += blockDim.x) {
+        Part o;
+        o.load_cg(s.part + t * kPartials);
+        acc.combine(o);
+    }
+    block_reduce(acc, sh);
+    if (threadIdx.x == 0) {
+        CaseState *cs = s.cstate + c;
+        double vnew = acc.vmax, rnew = acc.rmin;
+        if (!is_init) {
+            DevStats st;
+            st.dt = cs->dt;
+            st.flow_time = cs->t;
+            st.velmax = cs->velmax;
+            st.tau = P.CFL * P.maxEdge / jl_max(cs->velmax, 1.0e-6);
+            for (int v = 0; v < 4; ++v) { st.residual[v] = acc.res[v]; st.totals[v] = acc.tot[v]; }
+            st.rho_min = acc.rhomin;
+            st.rho_max = acc.rhomax;
+            st.kinetic_energy = acc.ek;
+            st.step = cs->step + 1;
+            st.nonfinite = acc.bad > 0.0 ? 1 : 0;
+            st.reserved0 = 0;
+            s.ring[(cs->step % s.ring_len) * m.ncases + c] = st;
+            cs->t = cs->t + cs->dt;
+            cs->step = cs->step + 1;
+            if (acc.bad > 0.0) cs->nonfinite = 1;
+        }
+        double dtn;
+        if (P.dt_mode == DT_REFERENCE_TAU) dtn = P.CFL * P.maxEdge / jl_max(vnew, 1.0e-6);
+        else if (P.dt_mode == DT_LOCAL_CFL) dtn = P.CFL * rnew;
+        else dtn = P.dt_fixed;
+        cs->dt = dtn;
+        cs->velmax = vnew;
+        cs->rmin = rnew;
+        cs->tiles_done = 0u;
+    }
+}
+
+// Publish the tile record and, if this tile completes its case, finalize it.
+__device__ __forceinline__ void tile_epilogue(const DevMesh &m, const DevState &s, int64_t tile, int c, Part &p,
+                                              Part *sh, bool is_init) {
+    __shared__ int s_last;
+    block_reduce(p, sh);
+    if (threadIdx.x == 0) {
+        p.store(s.part + tile * kPartials);
+        __threadfence();
+        const DevCase &P = m.cases[c];
+        unsigned int ntile = (unsigned int)(P.tile_end - P.tile_begin);
+        unsigned int prev = atomicAdd(&s.cstate[c].tiles_done, 1u);
+        s_last = (prev == ntile - 1u) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        finalize_case(m, s, c, sh, is_init);
+    }
+    __syncthreads();
+}
+
+// --------------------------------------------------------- MUSCL + flux
+
+// computeInterfaceSlope, computeslope2d.jl:3-136, for face k of cell g.
+template <int FLUX, bool QUAD>
+__device__ __forceinline__ void face_flux(const DevMesh &m, const DevCase &P, const double4 *__restrict__ pin,
+                                          const double4 *__restrict__ nodeP, int64_t g, int k, int nbk,
+                                          int dnk, int upk, int dn2k, int up2k, bool is_quad, const double *uL,
+                                          double hx_own, double t, double g2, double *f) {
+    const int64_t o = (int64_t)k * m.Nc + g;
+    const double side = m.len[o], nx = m.nx[o], ny = m.ny[o];
+    double uR[4], uUp[4], uDn[4];
+    double hxR = hx_own;
+    if (nbk >= 0) {
+        if (QUAD && is_quad) {
+            double4 a = nodeP[upk], a2 = nodeP[up2k], b = nodeP[dnk], b2 = nodeP[dn2k];
+            uUp[0] = 0.5 * (a.x + a2.x); uUp[1] = 0.5 * (a.y + a2.y);
+            uUp[2] = 0.5 * (a.z + a2.z); uUp[3] = 0.5 * (a.w + a2.w);
+            uDn[0] = 0.5 * (b.x + b2.x); uDn[1] = 0.5 * (b.y + b2.y);
+            uDn[2] = 0.5 * (b.z + b2.z); uDn[3] = 0.5 * (b.w + b2.w);
+        } else {
+            double4 a = nodeP[upk], b = nodeP[dnk];
+            uUp[0] = a.x; uUp[1] = a.y; uUp[2] = a.z; uUp[3] = a.w;
+            uDn[0] = b.x; uDn[1] = b.y; uDn[2] = b.z; uDn[3] = b.w;
+        }
+        double4 r = pin[nbk];
+        uR[0] = r.x; uR[1] = r.y; uR[2] = r.z; uR[3] = r.w;
+        if (P.limiter == LIM_VENKAT) hxR = m.hx[nbk];
+    } else {
+        bc_ghost<double>(P, m, -nbk - 1, g, k, uL, nx, ny, t, uR);
+        for (int v = 0; v < 4; ++v) { uDn[v] = uL[v]; uUp[v] = uR[v]; }
+    }
+    double UpL[4], UpR[4];
+    if (P.limiter == LIM_VENKAT) {
+        double KL = P.venkat_K * hx_own, KR = P.venkat_K * hxR;
+        double e2L = KL * KL * KL, e2R = KR * KR * KR;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            UpL[v] = uL[v] + 0.5 * lim_venkat(uL[v] - uDn[v], uR[v] - uL[v], e2L);
+            UpR[v] = uR[v] + 0.5 * lim_venkat(uR[v] - uUp[v], uL[v] - uR[v], e2R);
+        }
+    } else {
+        const int lk = P.limiter;
+        const double ksi = P.ksi;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            UpL[v] = uL[v] + 0.5 * limiter(lk, uL[v] - uDn[v], uR[v] - uL[v], ksi);
+            UpR[v] = uR[v] - 0.5 * limiter(lk, uR[v] - uL[v], uUp[v] - uR[v], ksi);
+        }
+    }
+    face_flux_fn<FLUX, double>(UpR, UpL, nx, ny, side, P.gamma, g2, f);
+}
+
+// Second Green-Gauss pass and transport model: the diffusion source of
+// calcDiffTerm (calcDiffTerm.jl:88-113; gradients per calcGradients.jl:36-139,
+// artificial viscosity per calcArtViscosity.jl:46-75).
+template <bool QUAD>
+__device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
+                                            bool is_quad, const double4 &me, double *diff) {
+    const int nf = (QUAD && is_quad) ? 4 : 3;
+    double sx[3] = {0.0, 0.0, 0.0}, sy[3] = {0.0, 0.0, 0.0};
+    double du = 0.0, dv = 0.0;
+    const bool art = (P.visc_model != VISC_REFERENCE) && P.art_visc;
+    for (int k = 0; k < nf; ++k) {
+        const int64_t o = (int64_t)k * m.Nc + g;
+        const double side = m.len[o], nx = m.nx[o], ny = m.ny[o];
+        const int2 e = m.c2n[o];
+        const NodeGrad A = s.nodeG[e.x], B = s.nodeG[e.y];
+        double fx, fy;
+        fx = 0.5 * (A.ru.x + B.ru.x) * -ny * side; fy = 0.5 * (A.ru.y + B.ru.y) * -nx * side;
+        sx[0] = (k == 0) ? fx : sx[0] + fx; sy[0] = (k == 0) ? fy : sy[0] + fy;
+        fx = 0.5 * (A.rv.x + B.rv.x) * -ny * side; fy = 0.5 * (A.rv.y + B.rv.y) * -nx * side;
+        sx[1] = (k == 0) ? fx : sx[1] + fx; sy[1] = (k == 0) ? fy : sy[1] + fy;
+        fx = 0.5 * (A.re.x + B.re.x) * -ny * side; fy = 0.5 * (A.re.y + B.re.y) * -nx * side;
+        sx[2] = (k == 0) ? fx : sx[2] + fx; sy[2] = (k == 0) ? fy : sy[2] + fy;
+        if (art) {
+            const double4 na = s.nodeP[e.x], nb = s.nodeP[e.y];
+            double fu = 0.5 * (na.y + nb.y) * -nx * side;
+            double fv = 0.5 * (na.z + nb.z) * -ny * side;
+            du = (k == 0) ? fu : du + fu;
+            dv = (k == 0) ? fv : dv + fv;
+        }
+    }
+    const double area = m.area[g];
+    double lap[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) lap[v] = sx[v] / area + sy[v] / area;
+    const double T = me.w / me.x / P.R;
+    diff[0] = 0.0;
+    if (P.visc_model == VISC_REFERENCE) {
+        const double mu = P.mu_ref;
+        diff[1] = mu * lap[0];
+        diff[2] = mu * lap[1];
+        diff[3] = mu * air_conductivity(T) * lap[2];
+    } else {
+        const double mu = (P.visc_model == VISC_SUTHERLAND) ? P.mu_ref * (sutherland(T) / P.suth_ref) : P.mu_ref;
+        double mart = 0.0;
+        if (art) {
+            const double HX = m.hx[g];
+            const double divU = du / area + dv / area;
+            const double aS = sqrt(P.gamma * me.w / me.x);
+            const double a = 0.05 * aS / HX / sqrt(2.0);
+            if (-divU > a) {
+                const double tmp = divU * divU - a * a;
+                if (tmp > 0.0) mart = 0.5 * me.x * HX / sqrt(2.0) * HX / sqrt(2.0) * sqrt(tmp) * 1.0e-5;
+            }
+        }
+        const double mue = mu + (P.art_visc ? mart : 0.0);
+        diff[1] = mue * lap[0];
+        diff[2] = mue * lap[1];
+        diff[3] = mue * P.gamma_over_Pr * lap[2];
+    }
+}
+
+// ---------------------------------------------------- fused cell kernel
+
+template <int FLUX, bool VISC, bool QUAD>
+__global__ void __launch_bounds__(256) k_cell_step(const DevMesh m, const DevState s) {
+    __shared__ Part sh[8];
+    const int par = *s.parity;
+    const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
+    double4 *__restrict__ pout = s.prim + (int64_t)(par ^ 1) * m.Nc;
+    const double4 *__restrict__ nodeP = s.nodeP;
+    for (int64_t tile = blockIdx.x; tile < m.ntiles; tile += gridDim.x) {
+        const int c = m.tile_case[tile];
+        const DevCase &P = m.cases[c];
+        const double dt = s.cstate[c].dt, t = s.cstate[c].t;
+        const int64_t g = tile * blockDim.x + threadIdx.x;
+        Part part;
+        part.init();
+        const int4 nb = m.nbr[g];
+        if (nb.x != kAbsent) {
+            const bool is_quad = QUAD && (nb.w != kAbsent);
+            const double4 me = pin[g];
+            const double uL[4] = {me.x, me.y, me.z, me.w};
+            const double gam = P.gamma;
+            const double g2 = 2.0 * (gam - 1.0) / (gam + 1.0);
+            const double hx_own = (P.limiter == LIM_VENKAT) ? m.hx[g] : 0.0;
+            const int4 dn = m.dn[g], up = m.up[g];
+            int4 dn2 = make_int4(0, 0, 0, 0), up2 = make_int4(0, 0, 0, 0);
+            if (QUAD && is_quad) { dn2 = m.dn2[g]; up2 = m.up2[g]; }
+            double F[4], f[4];
+            face_flux<FLUX, QUAD>(m, P, pin, nodeP, g, 0, nb.x, dn.x, up.x, dn2.x, up2.x, is_quad, uL, hx_own, t, g2, F);
+            face_flux<FLUX, QUAD>(m, P, pin, nodeP, g, 1, nb.y, dn.y, up.y, dn2.y, up2.y, is_quad, uL, hx_own, t, g2, f);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) F[v] = F[v] + f[v];
+            face_flux<FLUX, QUAD>(m, P, pin, nodeP, g, 2, nb.z, dn.z, up.z, dn2.z, up2.z, is_quad, uL, hx_own, t, g2, f);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) F[v] = F[v] + f[v];
+            if (QUAD && is_quad) {
+                face_flux<FLUX, QUAD>(m, P, pin, nodeP, g, 3, nb.w, dn.w, up.w, dn2.w, up2.w, is_quad, uL, hx_own, t, g2, f);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) F[v] = F[v] + f[v];
+            }
+            double diff[4] = {0.0, 0.0, 0.0, 0.0};
+            if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
+            // Euler update, calcOneStageMUSCLcpuFast.jl:94-99
+            const double rarea = m.rarea[g];
+            const double4 U = s.U[g];
+            const double Uo[4] = {U.x, U.y, U.z, U.w};
+            double Un[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Un[v] = (Uo[v] - F[v] * P.beta * dt * rarea + P.beta * dt * diff[v]);
+            s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
+            // updateVariablesSA, evaluate2d.jl:87-104
+            const double rho = Un[0];
+            const double ux = Un[1] / Un[0];
+            const double uy = Un[2] / Un[0];
+            const double p = (gam - 1.0) * (Un[3] - 0.5 * (Un[1] * Un[1] + Un[2] * Un[2]) / Un[0]);
+            const double a = sqrt(gam * p / rho);
+            const double vmax = sqrt(ux * ux + uy * uy) + a;
+            pout[g] = make_double4(rho, ux, uy, p);
+            const double area = m.area[g];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const double d = Un[v] - Uo[v];
+                part.res[v] = d * d;
+                part.tot[v] = Un[v] * area;
+            }
+            part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
+            part.vmax = vmax;
+            part.rmin = m.charlen[g] / vmax;
+            part.rhomin = me.x;
+            part.rhomax = me.x;
+            const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
+                            (p > 0.0);
+            part.bad = ok ? 0.0 : 1.0;
+        }
+        tile_epilogue(m, s, tile, c, part, sh, false);
+    }
+}
+
+// ------------------------------------------------------------ node kernel
+
+// cells2nodesSolutionReconstructionWithStencils (utilsFVM2dp.jl:299-365):
+// weighted primitive averages; with VISC also calcPhiInCellCluster's
+// unweighted means of rho u, rho v, E (calcGradients.jl:3-18) for the next
+// step's viscous term.  The last block flips the step parity.
+template <bool VISC, bool UNIT>
+__global__ void __launch_bounds__(256) k_node_avg(const DevMesh m, const DevState s, int flip, int zero_prims,
+                                                  int64_t n0, int64_t n1) {
+    const int par = *s.parity;
+    const double4 *__restrict__ src = s.prim + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
+    const int W = m.cluster_w;
+    for (int64_t J = n0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < n1; J += (int64_t)gridDim.x * blockDim.x) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, det = 0.0;
+        double c0 = 0.0, c1 = 0.0, c2 = 0.0;
+        int cnt = 0;
+        for (int j = 0; j < W; ++j) {
+            const int c = m.cl[(int64_t)j * m.Nn + J];
+            if (c >= 0) {
+                const double w = UNIT ? 1.0 : m.wt[(int64_t)j * m.Nn + J];
+                const double4 p = src[c];
+                a0 = a0 + p.x * w; a1 = a1 + p.y * w; a2 = a2 + p.z * w; a3 = a3 + p.w * w;
+                det = det + w;
+                if (VISC) {
+                    const double4 u = s.U[c];
+                    c0 = c0 + u.y; c1 = c1 + u.z; c2 = c2 + u.w;
+                    ++cnt;
+                }
+            }
+        }
+        if (det != 0.0) { a0 = a0 / det; a1 = a1 / det; a2 = a2 / det; a3 = a3 / det; }
+        s.nodeP[J] = zero_prims ? make_double4(0.0, 0.0, 0.0, 0.0) : make_double4(a0, a1, a2, a3);
+        if (VISC) {
+            if (cnt != 0) {
+                const double dc = (double)cnt;
+                s.nodeC[J] = make_double4(c0 / dc, c1 / dc, c2 / dc, 0.0);
+            } else {
+                s.nodeC[J] = make_double4(0.0, 0.0, 0.0, 0.0);
+            }
+        }
+    }
+    if (flip) {
+        __shared__ int s_last;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            unsigned int prev = atomicAdd(s.node_done, 1u);
+            s_last = (prev == gridDim.x - 1u) ? 1 : 0;
+        }
+        __syncthreads();
+        if (s_last && threadIdx.x == 0) {
+            *s.node_done = 0u;
+            *s.parity = par ^ 1;
+        }
+    }
+}
+
+// ------------------------------------------------------ viscous passes
+
+// First Green-Gauss gradient of rho u, rho v, E from the unweighted node
+// means (calcScalarFieldGreenGaussNodesBasedGradient, calcGradients.jl:36-139:
+// gradX pairs with -ny, gradY with -nx).
+template <bool QUAD>
+__global__ void __launch_bounds__(256) k_grad1_cells(const DevMesh m, const DevState s) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
+        const int4 nb = m.nbr[g];
+        if (nb.x == kAbsent) continue;
+        const int nf = (QUAD && nb.w != kAbsent) ? 4 : 3;
+        double sx[3] = {0.0, 0.0, 0.0}, sy[3] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < nf; ++k) {
+            const int64_t o = (int64_t)k * m.Nc + g;
+            const double side = m.len[o], nx = m.nx[o], ny = m.ny[o];
+            const int2 e = m.c2n[o];
+            const double4 A = s.nodeC[e.x], B = s.nodeC[e.y];
+            double fx, fy;
+            fx = 0.5 * (A.x + B.x) * -ny * side; fy = 0.5 * (A.x + B.x) * -nx * side;
+            sx[0] = (k == 0) ? fx : sx[0] + fx; sy[0] = (k == 0) ? fy : sy[0] + fy;
+            fx = 0.5 * (A.y + B.y) * -ny * side; fy = 0.5 * (A.y + B.y) * -nx * side;
+            sx[1] = (k == 0) ? fx : sx[1] + fx; sy[1] = (k == 0) ? fy : sy[1] + fy;
+            fx = 0.5 * (A.z + B.z) * -ny * side; fy = 0.5 * (A.z + B.z) * -nx * side;
+            sx[2] = (k == 0) ? fx : sx[2] + fx; sy[2] = (k == 0) ? fy : sy[2] + fy;
+        }
+        const double area = m.area[g];
+        NodeGrad r;
+        r.ru = make_double2(sx[0] / area, sy[0] / area);
+        r.rv = make_double2(sx[1] / area, sy[1] / area);
+        r.re = make_double2(sx[2] / area, sy[2] / area);
+        s.g1[g] = r;
+    }
+}
+
+// Unweighted node means of the first gradients (calcPhiInCellCluster on the
+// gradient fields, calcGradients.jl:3-18).
+__global__ void __launch_bounds__(256) k_grad1_nodes(const DevMesh m, const DevState s) {
+    const int W = m.cluster_w;
+    for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
+        double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int cnt = 0;
+        for (int j = 0; j < W; ++j) {
+            const int c = m.cl[(int64_t)j * m.Nn + J];
+            if (c >= 0) {
+                const NodeGrad q = s.g1[c];
+                v[0] = v[0] + q.ru.x; v[1] = v[1] + q.ru.y; v[2] = v[2] + q.rv.x;
+                v[3] = v[3] + q.rv.y; v[4] = v[4] + q.re.x; v[5] = v[5] + q.re.y;
+                ++cnt;
+            }
+        }
+        NodeGrad r;
+        if (cnt != 0) {
+            const double dc = (double)cnt;
+            r.ru = make_double2(v[0] / dc, v[1] / dc);
+            r.rv = make_double2(v[2] / dc, v[3] / dc);
+            r.re = make_double2(v[4] / dc, v[5] / dc);
+        } else {
+            r.ru = r.rv = r.re = make_double2(0.0, 0.0);
+        }
+        s.nodeG[J] = r;
+    }
+}
+
+// ------------------------------------------------------------ state init
+
+// phs2dcns2dcellsSA (utilsFVM2dp.jl:4-17) on the current primitives and the
+// reductions that give the first step's dt (createFields2d's VMAX).
+__global__ void __launch_bounds__(256) k_init_state(const DevMesh m, const DevState s, int64_t t0, int64_t t1) {
+    __shared__ Part sh[8];
+    const int par = *s.parity;
+    const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
+    for (int64_t tile = t0 + blockIdx.x; tile < t1; tile += gridDim.x) {
+        const int c = m.tile_case[tile];
+        const DevCase &P = m.cases[c];
+        const int64_t g = tile * blockDim.x + threadIdx.x;
+        Part part;
+        part.init();
+        const int4 nb = m.nbr[g];
+        if (nb.x != kAbsent) {
+            const double4 q = pin[g];
+            const double G = P.gamma;
+            const double r = q.x, u = q.y, v = q.z, pp = q.w;
+            s.U[g] = make_double4(r, r * u, r * v, pp / (G - 1.0) + 0.5 * r * (u * u + v * v));
+            const double a = sqrt(G * pp / r);
+            const double vmax = sqrt(u * u + v * v) + a;
+            part.vmax = vmax;
+            part.rmin = m.charlen[g] / vmax;
+        }
+        tile_epilogue(m, s, tile, c, part, sh, true);
+    }
+}
+
+}  // namespace gd2d

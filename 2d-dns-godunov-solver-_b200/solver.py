@@ -1,0 +1,198 @@
+"""Host-side mirror of the reference's solver interface over the C ABI.
+
+The reference drives one explicit step from Julia (testInviscidFluxesGPUx32.jl,
+testViscousFluxesTGV2d.jl): ``readMesh2dHDF5`` -> ``setupSolver_*.jl`` globals
+-> ``createFields2d`` -> a loop of ``calcDiffTerm`` /
+``calcOneStageMUSCLcpuFast`` / ``updateVariablesSA`` /
+``cells2nodesSolutionReconstructionWithStencils`` / residuals.  Here the same
+call shape maps onto libgodunov2d.so:
+
+  setupSolver(meshes, cfgs)            -> Solver (gd2d_setup)
+  Solver.createFields2d(i, rho,u,v,p)  -> gd2d_set_state
+  Solver.propagate2d(nsteps)           -> gd2d_propagate (the whole loop body)
+  Solver.calcOneStageMUSCLcpuFast(...) -> gd2d_calc_one_stage
+  Solver.updateVariablesSA(i)          -> gd2d_update_variables
+  Solver.cells2nodesSolutionReconstructionWithStencils() -> gd2d_cells_to_nodes
+  Solver.calcDiffTerm(i)               -> gd2d_calc_diff_term
+
+Every call runs on the GPU; there is no CPU fallback.  Arrays are numpy in
+the reference's column-major layout.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+from .mesh import Mesh2d
+
+
+def mesh_view(mesh: Mesh2d) -> N.MeshView:
+    v = N.MeshView()
+    v.n_cells, v.n_nodes, v.n_neib_cells = mesh.nCells, mesh.nNodes, mesh.nNeibCells
+    v.x_nodes = mesh.xNodes.ctypes.data
+    v.y_nodes = mesh.yNodes.ctypes.data
+    for name in ("mesh_connectivity", "cell_stiffness", "cells2nodes", "cell_edges_Nx", "cell_edges_Ny",
+                 "cell_edges_length", "cell_areas", "HX", "cell_mid_points", "cell_clusters", "node_stencils",
+                 "node2cellL2up", "node2cellL2down"):
+        setattr(v, name, getattr(mesh, name).ctypes.data)
+    return v
+
+
+def make_params(cfg: Dict) -> N.Params:
+    """gd2d_params from a case configuration dict (see cases.py)."""
+    p = N.Params()
+    th = cfg["thermo"]
+    p.RGAS, p.Gamma = th["RGAS"], th["Gamma"]
+    p.Cp, p.mu, p.kGas = th.get("Cp", 1000.0), th.get("mu", 0.0), th.get("kGas", 0.0)
+    p.CFL = cfg.get("CFL", 0.5)
+    p.dt = cfg.get("dt", 0.0)
+    p.beta = cfg.get("beta", 1.0)
+    p.ksi = cfg.get("ksi", 1.0e-12)
+    p.venkat_K = cfg.get("venkat_K", 5.0)
+    p.mu_ref = cfg.get("mu_ref", 0.0)
+    p.T_ref = cfg.get("T_ref", 300.0)
+    p.Pr = cfg.get("Pr", 0.72)
+    tgv = cfg.get("tgv", {})
+    p.tgv_U0, p.tgv_P0 = tgv.get("U0", 40.0), tgv.get("P0", 100000.0)
+    p.tgv_L, p.tgv_mu = tgv.get("L", 1.0), tgv.get("mu", 1.0e-2)
+    p.start_time = cfg.get("start_time", 0.0)
+    p.flux = N.FLUX[cfg.get("flux", "ausm")]
+    p.limiter = N.LIMITER[cfg.get("limiter", "minmod")]
+    p.viscosity = N.VISC[cfg.get("viscosity", "none")]
+    p.art_viscosity = int(cfg.get("art_viscosity", 0))
+    p.dt_mode = int(cfg.get("dt_mode", 1))
+    p.init_nodes = int(cfg.get("init_nodes", 0))
+    bcs = cfg.get("bc", [])
+    if len(bcs) > N.GD2D_MAX_BC:
+        raise ValueError("too many boundary kinds")
+    p.n_bc = len(bcs)
+    for i, b in enumerate(bcs):
+        p.bc[i].tag, p.bc[i].kind = b["tag"], N.BC_KIND[b["kind"]]
+        p.bc[i].rho, p.bc[i].u, p.bc[i].v, p.bc[i].p = (b.get("rho", 0.0), b.get("u", 0.0), b.get("v", 0.0),
+                                                        b.get("p", 0.0))
+        p.bc[i].Tw = b.get("Tw", 0.0)
+    return p
+
+
+def make_launch(precision="f64", order="hilbert", loop="cell", block=0, node_block=0, persistent=0,
+                graph_steps=0, stream=None) -> N.Launch:
+    l = N.Launch()
+    l.precision = N.PRECISION[precision] if isinstance(precision, str) else int(precision)
+    l.order = N.ORDER[order] if isinstance(order, str) else int(order)
+    l.loop = N.LOOP[loop] if isinstance(loop, str) else int(loop)
+    l.block, l.node_block, l.persistent, l.graph_steps = block, node_block, persistent, graph_steps
+    l.stream = stream
+    return l
+
+
+class Solver:
+    """One gd2d handle: several independent cases advancing together."""
+
+    def __init__(self, meshes: Sequence[Mesh2d], cfgs: Sequence[Dict], launch: Optional[N.Launch] = None):
+        self.L = N.load()
+        self.meshes = list(meshes)
+        self.cfgs = [dict(c) for c in cfgs]
+        n = len(self.meshes)
+        self._views = (N.MeshView * n)(*[mesh_view(m) for m in self.meshes])
+        self._params = (N.Params * n)(*[make_params(c) for c in self.cfgs])
+        self._launch = launch if launch is not None else make_launch()
+        h = C.c_void_p()
+        N.check(self.L.gd2d_setup(C.byref(h), n, self._views, self._params, C.byref(self._launch)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.gd2d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ncases(self):
+        return len(self.meshes)
+
+    def _chk(self, code):
+        return N.check(code, self.h)
+
+    # -- initial / restart state -------------------------------------------
+    def createFields2d(self, icase: int, rho, ux, uy, p):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, ux, uy, p)]
+        for a in arrs:
+            if a.shape != (self.meshes[icase].nCells,):
+                raise ValueError("field size does not match the mesh")
+        dp = C.POINTER(C.c_double)
+        self._chk(self.L.gd2d_set_state(self.h, icase, *[a.ctypes.data_as(dp) for a in arrs]))
+
+    set_state = createFields2d
+
+    def set_conservative(self, icase: int, ucons, flow_time: float, rebuild_nodes: bool = True):
+        u = np.asfortranarray(ucons, dtype=np.float64)
+        self._chk(self.L.gd2d_set_conservative(self.h, icase, u.ctypes.data_as(C.POINTER(C.c_double)),
+                                               float(flow_time), int(rebuild_nodes)))
+
+    # -- stepping ------------------------------------------------------------
+    def propagate2d(self, nsteps: int) -> List[Dict]:
+        st = (N.Stats * self.ncases)()
+        self._chk(self.L.gd2d_propagate(self.h, int(nsteps), st))
+        return [s.as_dict() for s in st]
+
+    propagate = propagate2d
+
+    def history(self, icase: int, capacity: int = 1 << 20) -> List[Dict]:
+        buf = (N.Stats * capacity)()
+        n = self._chk(self.L.gd2d_get_history(self.h, icase, buf, capacity))
+        return [buf[i].as_dict() for i in range(n)]
+
+    def get_state(self, icase: int) -> Dict[str, np.ndarray]:
+        m = self.meshes[icase]
+        U = np.zeros((m.nCells, 4), order="F")
+        P = np.zeros((m.nCells, 4), order="F")
+        Nd = np.zeros((m.nNodes, 4), order="F")
+        dp = C.POINTER(C.c_double)
+        self._chk(self.L.gd2d_get_state(self.h, icase, U.ctypes.data_as(dp), P.ctypes.data_as(dp),
+                                        Nd.ctypes.data_as(dp)))
+        return {"Ucons": U, "prims": P, "node_prims": Nd}
+
+    def last_timing(self) -> Tuple[float, float, int]:
+        t, c, n = C.c_double(), C.c_double(), C.c_int64()
+        self._chk(self.L.gd2d_last_timing(self.h, C.byref(t), C.byref(c), C.byref(n)))
+        return t.value, c.value, n.value
+
+    # -- the reference's functions one at a time ---------------------------------
+    def calcOneStageMUSCLcpuFast(self, icase: int, beta: float, dt: float, flow_time: float):
+        m = self.meshes[icase]
+        F = np.zeros((m.nCells, 4), order="F")
+        Un = np.zeros((m.nCells, 4), order="F")
+        dp = C.POINTER(C.c_double)
+        self._chk(self.L.gd2d_calc_one_stage(self.h, icase, beta, dt, flow_time, F.ctypes.data_as(dp),
+                                             Un.ctypes.data_as(dp)))
+        return F, Un
+
+    def updateVariablesSA(self, icase: int):
+        m = self.meshes[icase]
+        D = np.zeros((m.nCells, 4), order="F")
+        self._chk(self.L.gd2d_update_variables(self.h, icase, D.ctypes.data_as(C.POINTER(C.c_double))))
+        return D
+
+    def cells2nodesSolutionReconstructionWithStencils(self):
+        self._chk(self.L.gd2d_cells_to_nodes(self.h))
+
+    def calcDiffTerm(self, icase: int):
+        m = self.meshes[icase]
+        D = np.zeros((m.nCells, 4), order="F")
+        self._chk(self.L.gd2d_calc_diff_term(self.h, icase, D.ctypes.data_as(C.POINTER(C.c_double))))
+        return D
+
+
+def setupSolver(meshes, cfgs, **launch_kw) -> Solver:
+    """setupSolver_*.jl + device setup for one or more cases."""
+    if isinstance(meshes, Mesh2d):
+        meshes, cfgs = [meshes], [cfgs]
+    return Solver(meshes, cfgs, make_launch(**launch_kw))

@@ -1,0 +1,288 @@
+"""Benchmark of the explicit Godunov step on B200.
+
+Default workload (one GPU): the plain-FP64 viscous supersonic cylinder,
+[-5,15]x[-8,8] on a 1025^2 node grid, triangulated, cells inside r<0.5
+removed (~2.09M cells), M=3.5, Re_D=1e4, Sutherland + artificial viscosity,
+Venkatakrishnan limiter, AUSM+, local-CFL 0.4.  A "step" is one explicit
+time step over all cells.  Synthetic, seeded inputs (no dataset exists).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--config cylinder|square|tgv_batch|cyl_batch] [--precision f64|mixed]
+
+value: cell-steps/s (Mcell-steps/s) with state resident in HBM, device
+time from CUDA events on the solver's stream, max over ranks.  The working
+set (~0.9 GB) is far larger than L2, so no flush is needed between steps.
+e2e: the same metric through the C ABI with host buffers: set_state from
+pinned host memory, K x gd2d_propagate(h, 1, stats) (per-step stats read
+back), gd2d_get_state of the final state.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+import __graft_entry__ as graft  # noqa: E402
+
+# Algorithmic bytes per cell-step (compulsory traffic of the reference
+# dataflow: state read+write, face geometry, connectivity, node-average
+# cluster data; intermediates counted zero).
+ALG_BYTES = {("f64", False): 216, ("f64", True): 248, ("mixed", False): 164, ("mixed", True): 192}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_workload(pkg, config: str, precision: str):
+    C = pkg.cases
+    if config == "square":
+        mesh, cfg, prims = C.square_inviscid(101)
+        cfg = dict(cfg, dt_mode=2)
+        items = [(mesh, cfg, prims)]
+        desc = {"workload": "square_inviscid_fp64", "mesh": "unit square 101x101 nodes, jittered tris",
+                "cells": mesh.nCells}
+    elif config == "tgv_batch":
+        items = C.batched_tgv(64)
+        desc = {"workload": "batched_tgv_64", "cases": 64, "cells": sum(m.nCells for m, _, _ in items)}
+    elif config == "cyl_batch":
+        items = C.batched_cylinders(16)
+        desc = {"workload": "batched_cylinders_16", "cases": 16, "cells": sum(m.nCells for m, _, _ in items)}
+    else:
+        mesh, cfg, prims = C.cylinder_case(1025)
+        cfg = dict(cfg, dt_mode=2)
+        items = [(mesh, cfg, prims)]
+        desc = {"workload": "cylinder_viscous_fp64" if precision == "f64" else "cylinder_viscous_mixed",
+                "mesh": "[-5,15]x[-8,8] 1025^2 nodes, tris, r<0.5 removed", "cells": mesh.nCells,
+                "mach": 3.5, "re_d": 1.0e4, "limiter": "venkatakrishnan", "viscosity": "sutherland+artificial"}
+    viscous = items[0][1].get("viscosity", "none") != "none"
+    return items, desc, viscous
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+        dist = td
+    return world, rank, local, dist
+
+
+def dist_max(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_reference(pkg, items, steps, warmup, budget_s=25.0):
+    """Time the CPU restatement of the reference step (oracle, all host
+    threads) on a bounded sample of the workload."""
+    from oracle import oracle as orc
+    orc.build()
+    nthreads = os.cpu_count() or 1
+    mesh, cfg, prims = items[0]
+    o = orc.Oracle(mesh, cfg, nthreads=nthreads)
+    o.init_fields(*prims)
+    t0 = time.perf_counter()
+    o.step()
+    t1 = time.perf_counter() - t0
+    nsteps = max(1, min(steps, int(budget_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        o.step()
+    dt = time.perf_counter() - t0
+    cells = mesh.nCells
+    return {"value": cells * nsteps / dt / 1e6, "unit": "Mcell-steps/s", "cores": nthreads, "kind": "port",
+            "sample": f"{nsteps} steps of case 0 ({cells} cells) after 1 warm-up step, {nthreads} threads",
+            "seconds": dt}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="cylinder", choices=["cylinder", "square", "tgv_batch", "cyl_batch"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
+    ap.add_argument("--order", default="hilbert")
+    ap.add_argument("--graph-steps", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local, dist = dist_setup(args)
+    pkg = graft.load_package()
+    items, desc, viscous = build_workload(pkg, args.config, args.precision)
+    metric = "Mcell-steps/s"
+    cfg_line = dict(desc, precision=args.precision, parallelism=("replicas%d" % world), l2_flush="inputs > L2")
+
+    if args.impl == "reference":
+        if rank != 0:
+            dist_barrier(dist)
+            return
+        cb = cpu_reference(pkg, items, args.steps, args.warmup, budget_s=60.0)
+        line = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": cb["unit"], "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg_line,
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        dist_barrier(dist)
+        return
+
+    meshes = [m for m, _, _ in items]
+    cfgs = [c for _, c, _ in items]
+    launch = pkg.solver.make_launch(precision=args.precision, order=args.order, graph_steps=args.graph_steps)
+    s = pkg.solver.Solver(meshes, cfgs, launch)
+    for i, (_, _, p) in enumerate(items):
+        s.createFields2d(i, *p)
+    cells = sum(m.nCells for m in meshes)
+
+    # warm-up
+    s.propagate2d(args.warmup)
+    dist_barrier(dist)
+    with ClockSampler(local) as clk:
+        s.propagate2d(args.steps)
+        total_ms, cell_ms, launches = s.last_timing()
+    dist_barrier(dist)
+    total_ms = dist_max(dist, total_ms)
+    clocks = clk.summary()
+    value = cells * args.steps * world / (total_ms / 1e3) / 1e6
+    ms_per_step = total_ms / args.steps
+
+    # end to end through the C ABI with host buffers
+    import ctypes as C
+    N = pkg._native
+    L = N.load()
+    m0 = meshes[0]
+    host_prims = [np.ascontiguousarray(x, dtype=np.float64) for x in items[0][2]]
+    ucons = np.zeros((m0.nCells, 4), order="F")
+    st = (N.Stats * len(meshes))()
+    dp = C.POINTER(C.c_double)
+    dist_barrier(dist)
+    e2e_steps = args.steps
+    t0 = time.perf_counter()
+    N.check(L.gd2d_set_state(s.h, 0, *[a.ctypes.data_as(dp) for a in host_prims]), s.h)
+    for _ in range(e2e_steps):
+        N.check(L.gd2d_propagate(s.h, 1, st), s.h)
+    N.check(L.gd2d_get_state(s.h, 0, ucons.ctypes.data_as(dp), None, None), s.h)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = dist_max(dist, e2e_s)
+    e2e_val = m0.nCells * e2e_steps * world / e2e_s / 1e6
+    h2d = 4 * 8 * m0.nCells / e2e_steps
+    d2h = C.sizeof(N.Stats) * len(meshes) + 4 * 8 * m0.nCells / e2e_steps
+
+    peak, peak_kind = load_peaks()
+    alg = ALG_BYTES[(args.precision, viscous)]
+    achieved = alg * cells / (cell_ms / 1e3) / 1e9 if cell_ms > 0 else None
+    step_achieved = alg * cells / (ms_per_step / 1e3) / 1e9
+    line = {"metric": metric, "value": value, "unit": "Mcell-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "f64" else "f32+f64",
+            "data": "synthetic (seeded generated meshes and initial states)", "config": cfg_line,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "kernel": "k_cell_step (fused reconstruction+flux+update)",
+                         "alg_bytes_per_cell": alg, "cell_kernel_ms": cell_ms, "peak_kind": peak_kind,
+                         "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak},
+            "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches), "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference(pkg, items, args.steps, args.warmup)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

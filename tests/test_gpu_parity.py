@@ -1,0 +1,193 @@
+"""GPU parity: the CUDA step through the C ABI against the CPU oracle.
+
+Tolerance (north star): FP64 within 1e-12 relative per step and 1e-10
+after 100 steps, measured per variable as max|gpu - oracle| / max|oracle|.
+The FP64 kernels are built without multiply-add contraction, so most
+fields are expected to match bit for bit; the tests report that too.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-12
+TOL_100 = 1e-10
+
+
+def relerr(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if a.ndim == 1:
+        a, b = a[:, None], b[:, None]
+    scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
+    return float((np.abs(a - b).max(axis=0) / scale).max())
+
+
+def run_pair(pkg, orc, mesh, cfg, prims, nsteps, **launch):
+    s = pkg.setupSolver(mesh, cfg, **launch)
+    s.createFields2d(0, *prims)
+    o = orc.Oracle(mesh, cfg, nthreads=4)
+    o.init_fields(*prims)
+    gh, oh = [], []
+    for _ in range(nsteps):
+        gh.append(s.propagate2d(1)[0])
+        oh.append(o.step())
+    return s, o, gh, oh
+
+
+def compare_state(s, o, icase=0):
+    g = s.get_state(icase)
+    eU = relerr(g["Ucons"], o.field("Uold"))
+    eP = relerr(g["prims"], o.prims())
+    eN = relerr(g["node_prims"], o.node_prims())
+    bit = bool(np.array_equal(g["Ucons"], o.field("Uold")))
+    return eU, eP, eN, bit
+
+
+def compare_stats(gh, oh, tol):
+    for a, b in zip(gh, oh):
+        assert a["dt"] == pytest.approx(b["dt"], rel=tol, abs=0)
+        assert a["flowTime"] == pytest.approx(b["flowTime"], rel=tol, abs=1e-300)
+        for v in range(4):
+            assert a["residual"][v] == pytest.approx(b["residual"][v], rel=1e-10, abs=1e-300)
+        assert a["rhoMin"] == b["rhoMin"] and a["rhoMax"] == b["rhoMax"]
+        assert a["nonfinite"] == 0 and b["nonfinite"] == 0
+
+
+def test_square_inviscid_step_and_100(pkg, orc):
+    mesh, cfg, prims = pkg.cases.square_inviscid(101)
+    cfg = dict(cfg, dt_mode=2)
+    s, o, gh, oh = run_pair(pkg, orc, mesh, cfg, prims, 1)
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_STEP, (eU, eP, eN)
+    assert bit, "FP64 path expected bit-identical to the oracle after one step"
+    for _ in range(99):
+        gh.append(s.propagate2d(1)[0])
+        oh.append(o.step())
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_100, (eU, eP, eN)
+    compare_stats(gh, oh, 1e-12)
+
+
+@pytest.mark.parametrize("order", ["natural", "hilbert", "rcm"])
+def test_ordering_is_bit_exact(pkg, orc, order):
+    mesh, cfg, prims = pkg.cases.square_inviscid(41)
+    cfg = dict(cfg, dt_mode=2)
+    s, o, gh, oh = run_pair(pkg, orc, mesh, cfg, prims, 10, order=order)
+    eU, eP, eN, bit = compare_state(s, o)
+    assert bit and eN == 0.0, (order, eU, eP, eN)
+
+
+def test_graph_replay_equals_eager(pkg):
+    mesh, cfg, prims = pkg.cases.square_inviscid(41)
+    cfg = dict(cfg, dt_mode=2)
+    out = []
+    for gsteps in (1, 8):
+        s = pkg.setupSolver(mesh, cfg, graph_steps=gsteps)
+        s.createFields2d(0, *prims)
+        s.propagate2d(24)
+        out.append(s.get_state(0)["Ucons"])
+        hist = s.history(0)
+        assert len(hist) == 24 and hist[-1]["step"] == 24
+        s.close()
+    assert np.array_equal(out[0], out[1])
+
+
+def test_reference_tgv_viscous(pkg, orc):
+    """The reference's own viscous TGV setup: calcDiffTerm as written
+    (constant mu, air conductivity) and the analytic TGV ghost state."""
+    mesh, cfg, prims = pkg.cases.reference_tgv_case(41)
+    s, o, gh, oh = run_pair(pkg, orc, mesh, cfg, prims, 1)
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_STEP, (eU, eP, eN)
+    for _ in range(29):
+        gh.append(s.propagate2d(1)[0])
+        oh.append(o.step())
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_100, (eU, eP, eN)
+
+
+def test_cylinder_sutherland_artvisc_venkat(pkg, orc):
+    mesh, cfg, prims = pkg.cases.cylinder_case(65, radius=0.5)
+    cfg = dict(cfg, dt_mode=2)
+    s, o, gh, oh = run_pair(pkg, orc, mesh, cfg, prims, 1)
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_STEP, (eU, eP, eN)
+    for _ in range(39):
+        gh.append(s.propagate2d(1)[0])
+        oh.append(o.step())
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_100, (eU, eP, eN)
+    compare_stats(gh, oh, 1e-12)
+
+
+@pytest.mark.parametrize("flux", ["roe", "ausm_m2020"])
+def test_other_fluxes(pkg, orc, flux):
+    mesh, cfg, prims = pkg.cases.square_inviscid(41, flux=flux)
+    cfg = dict(cfg, dt_mode=2)
+    s, o, gh, oh = run_pair(pkg, orc, mesh, cfg, prims, 20)
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_100, (flux, eU, eP, eN)
+
+
+@pytest.mark.parametrize("limiter", ["vanleer", "vanalbada", "none", "venkat"])
+def test_other_limiters(pkg, orc, limiter):
+    mesh, cfg, prims = pkg.cases.square_inviscid(41, limiter=limiter)
+    cfg = dict(cfg, dt_mode=2, CFL=0.3)
+    s, o, gh, oh = run_pair(pkg, orc, mesh, cfg, prims, 10)
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_100, (limiter, eU, eP, eN)
+
+
+def test_quad_mesh(pkg, orc):
+    mesh = pkg.mesh.structured_mesh(33, 25, 0.0, 1.0, 0.0, 0.75, quads=True)
+    _, cfg, _ = pkg.cases.square_inviscid(5)
+    xc, yc = mesh.cell_mid_points[:, 0], mesh.cell_mid_points[:, 1]
+    rho = 1.0 + 0.2 * np.exp(-((xc - 0.3) ** 2 + (yc - 0.4) ** 2) / 0.005)
+    n = mesh.nCells
+    prims = (rho, np.full(n, 2.0), np.full(n, 0.1), np.full(n, 1.0 / 1.4))
+    cfg = dict(cfg, dt_mode=2, CFL=0.4)
+    s, o, gh, oh = run_pair(pkg, orc, mesh, cfg, prims, 20)
+    eU, eP, eN, bit = compare_state(s, o)
+    assert max(eU, eP, eN) <= TOL_100, (eU, eP, eN)
+
+
+def test_batched_cases_match_individual_oracles(pkg, orc):
+    specs = [pkg.cases.square_inviscid(21, seed=2), pkg.cases.tgv_case(26, 0.3, 400.0),
+             pkg.cases.square_inviscid(37, seed=3)]
+    # viscosity must agree inside a handle: run the inviscid ones together
+    inv = [specs[0], specs[2]]
+    meshes = [m for m, _, _ in inv]
+    cfgs = [dict(c, dt_mode=2) for _, c, _ in inv]
+    s = pkg.solver.Solver(meshes, cfgs, pkg.solver.make_launch())
+    for i, (_, _, p) in enumerate(inv):
+        s.createFields2d(i, *p)
+    s.propagate2d(15)
+    for i, (m, c, p) in enumerate(inv):
+        o = orc.Oracle(m, dict(c, dt_mode=2), nthreads=2)
+        o.init_fields(*p)
+        o.run(15)
+        g = s.get_state(i)
+        assert np.array_equal(g["Ucons"], o.field("Uold")), i
+    # a batch of viscous TGV cases of different sizes
+    tg = [pkg.cases.tgv_case(n, 0.2 + 0.05 * k, 300.0 + 100 * k) for k, n in enumerate((17, 30, 23))]
+    s2 = pkg.solver.Solver([m for m, _, _ in tg], [c for _, c, _ in tg], pkg.solver.make_launch())
+    for i, (_, _, p) in enumerate(tg):
+        s2.createFields2d(i, *p)
+    s2.propagate2d(12)
+    for i, (m, c, p) in enumerate(tg):
+        o = orc.Oracle(m, c, nthreads=2)
+        o.init_fields(*p)
+        o.run(12)
+        assert relerr(s2.get_state(i)["Ucons"], o.field("Uold")) <= TOL_100, i
+
+
+def test_nonfinite_state_is_reported(pkg):
+    mesh, cfg, prims = pkg.cases.square_inviscid(21)
+    rho, u, v, p = [np.array(x, dtype=np.float64) for x in prims]
+    p[5] = -1.0  # inadmissible pressure: the step must report it, not fault
+    s = pkg.setupSolver(mesh, dict(cfg, dt_mode=0, dt=1e-4))
+    s.createFields2d(0, rho, u, v, p)
+    with pytest.raises(pkg._native.NativeError) as ei:
+        s.propagate2d(3)
+    assert ei.value.code == -4

