@@ -79,6 +79,9 @@ struct gd2d_handle {
     cudaEvent_t ev_total[2] = {nullptr, nullptr};
     double last_total_ms = 0.0, last_cell_ms = 0.0;
     int64_t last_launches = 0;
+    double4 *pinned = nullptr;  // page-locked staging for state uploads and downloads
+    size_t pinned_count = 0;
+    std::vector<CaseState> cs_host;
     std::string err;
 };
 
@@ -572,9 +575,31 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         (void)per_sm;
     }
     h->history.assign(n_cases, {});
+    h->cs_host.assign(n_cases, CaseState{});
     cudaEventCreate(&h->ev_total[0]);
     cudaEventCreate(&h->ev_total[1]);
+    size_t maxn = 1;
+    for (auto &c : h->cases) maxn = std::max<size_t>(maxn, std::max(c.nc, c.nn));
+    {
+        cudaError_t e = cudaMallocHost((void **)&h->pinned, maxn * sizeof(double4));
+        if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaMallocHost: %s", cudaGetErrorString(e)));
+        h->pinned_count = maxn;
+    }
+    // uploads above went through the legacy stream; finish them before any
+    // work is queued on the handle's stream
+    {
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_CUDA, "setup: %s", cudaGetErrorString(e)));
+    }
     *out = h;
+    return GD2D_OK;
+}
+
+// Stream-ordered copies on the handle's stream (the handle's stream does not
+// synchronise with the legacy default stream).
+static int copy_sync(gd2d_handle *h, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+    CUDA_TRY(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return GD2D_OK;
 }
 
@@ -591,20 +616,21 @@ static int drop_graph(gd2d_handle *h) {
     return GD2D_OK;
 }
 
-// Upload cell primitives (reference order) of one case and rebuild U, the
-// node fields and the first dt of that case.
-static int init_case_from_prims(gd2d_handle *h, int32_t icase, const std::vector<double4> &prims_new_order,
-                                double t0, bool nodes_from_cells) {
+// The cell primitives of one case, already permuted into the pinned staging
+// buffer, become the case's state: U, the node fields and the first dt.
+static int init_case_from_pinned(gd2d_handle *h, int32_t icase, double t0, bool nodes_from_cells) {
     HostCase &hc = h->cases[icase];
     cudaSetDevice(h->device);
     int par = 0;
-    CUDA_TRY(h, cudaMemcpy(&par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost));
-    CUDA_TRY(h, cudaMemcpy(h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, prims_new_order.data(),
-                           sizeof(double4) * hc.nc, cudaMemcpyHostToDevice));
-    CaseState cs{};
+    int rc = copy_sync(h, &par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost);
+    if (rc) return rc;
+    CUDA_TRY(h, cudaMemcpyAsync(h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, h->pinned, sizeof(double4) * hc.nc,
+                                cudaMemcpyHostToDevice, h->stream));
+    CaseState &cs = h->cs_host[icase];
+    cs = CaseState{};
     cs.t = t0;
-    CUDA_TRY(h, cudaMemcpy(h->s.cstate + icase, &cs, sizeof cs, cudaMemcpyHostToDevice));
-    // Per-case init restricted to this case's tiles and nodes.
+    CUDA_TRY(h, cudaMemcpyAsync(h->s.cstate + icase, &cs, sizeof cs, cudaMemcpyHostToDevice, h->stream));
+    // per-case init restricted to this case's tiles and nodes
     const DevCase &d = h->hcases[icase];
     CUDA_TRY(h, launch_init_state_f64(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
     CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off, hc.node_off + hc.nn,
@@ -624,12 +650,12 @@ int gd2d_set_state(gd2d_handle *h, int32_t icase, const double *density, const d
     if (rc) return rc;
     if (!density || !ux || !uy || !pressure) return fail(h, GD2D_ERR_ARG, "NULL field pointer");
     HostCase &hc = h->cases[icase];
-    std::vector<double4> pr(hc.nc);
+    double4 *pr = h->pinned;
     for (int64_t j = 0; j < hc.nc; ++j) {
         int64_t i = hc.cell_perm[j];
         pr[j] = make_double4(density[i], ux[i], uy[i], pressure[i]);
     }
-    return init_case_from_prims(h, icase, pr, hc.start_time, hc.params.init_nodes != 0);
+    return init_case_from_pinned(h, icase, hc.start_time, hc.params.init_nodes != 0);
 }
 
 int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, double flow_time, int32_t rebuild_nodes) {
@@ -638,14 +664,14 @@ int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, do
     if (!ucons) return fail(h, GD2D_ERR_ARG, "NULL ucons");
     HostCase &hc = h->cases[icase];
     const double G = hc.params.Gamma;
-    std::vector<double4> pr(hc.nc);
+    double4 *pr = h->pinned;
     for (int64_t j = 0; j < hc.nc; ++j) {
         int64_t i = hc.cell_perm[j];
         double U1 = ucons[cidx(hc.nc, i, 0)], U2 = ucons[cidx(hc.nc, i, 1)], U3 = ucons[cidx(hc.nc, i, 2)],
                U4 = ucons[cidx(hc.nc, i, 3)];
         pr[j] = make_double4(U1, U2 / U1, U3 / U1, (G - 1.0) * (U4 - 0.5 * (U2 * U2 + U3 * U3) / U1));
     }
-    return init_case_from_prims(h, icase, pr, flow_time, rebuild_nodes != 0);
+    return init_case_from_pinned(h, icase, flow_time, rebuild_nodes != 0);
 }
 
 static int capture_graph(gd2d_handle *h, int steps, bool timing) {
@@ -685,7 +711,8 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
     while (done < nsteps) {
         const int32_t chunk = std::min<int32_t>(nsteps - done, h->s.ring_len);
         std::vector<CaseState> before(h->ncases);
-        CUDA_TRY(h, cudaMemcpy(before.data(), h->s.cstate, sizeof(CaseState) * h->ncases, cudaMemcpyDeviceToHost));
+        int rc0 = copy_sync(h, before.data(), h->s.cstate, sizeof(CaseState) * h->ncases, cudaMemcpyDeviceToHost);
+        if (rc0) return rc0;
         CUDA_TRY(h, cudaEventRecord(h->ev_total[0], h->stream));
         int32_t k = 0;
         bool used_graph = false;
@@ -722,8 +749,18 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
             }
         }
         // history
+        // the chunk's ring rows (the ring is [ring_len][ncases]; rows wrap)
         std::vector<DevStats> ring((size_t)h->s.ring_len * h->ncases);
-        CUDA_TRY(h, cudaMemcpy(ring.data(), h->s.ring, sizeof(DevStats) * ring.size(), cudaMemcpyDeviceToHost));
+        {
+            const int64_t r0 = before[0].step % h->s.ring_len;
+            const int64_t first = std::min<int64_t>(chunk, h->s.ring_len - r0);
+            CUDA_TRY(h, cudaMemcpyAsync(ring.data() + r0 * h->ncases, h->s.ring + r0 * h->ncases,
+                                        sizeof(DevStats) * first * h->ncases, cudaMemcpyDeviceToHost, h->stream));
+            if (first < chunk)
+                CUDA_TRY(h, cudaMemcpyAsync(ring.data(), h->s.ring, sizeof(DevStats) * (chunk - first) * h->ncases,
+                                            cudaMemcpyDeviceToHost, h->stream));
+            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+        }
         bool bad = false;
         for (int c = 0; c < h->ncases; ++c) {
             for (int32_t q = 0; q < chunk; ++q) {
@@ -761,12 +798,13 @@ int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, 
     if (rc) return rc;
     cudaSetDevice(h->device);
     HostCase &hc = h->cases[icase];
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     int par = 0;
-    CUDA_TRY(h, cudaMemcpy(&par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost));
-    std::vector<double4> tmp(std::max(hc.nc, hc.nn));
+    rc = copy_sync(h, &par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost);
+    if (rc) return rc;
+    double4 *tmp = h->pinned;
     if (ucons) {
-        CUDA_TRY(h, cudaMemcpy(tmp.data(), h->s.U + hc.cell_off, sizeof(double4) * hc.nc, cudaMemcpyDeviceToHost));
+        rc = copy_sync(h, tmp, h->s.U + hc.cell_off, sizeof(double4) * hc.nc, cudaMemcpyDeviceToHost);
+        if (rc) return rc;
         for (int64_t j = 0; j < hc.nc; ++j) {
             int64_t i = hc.cell_perm[j];
             ucons[cidx(hc.nc, i, 0)] = tmp[j].x; ucons[cidx(hc.nc, i, 1)] = tmp[j].y;
@@ -774,8 +812,9 @@ int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, 
         }
     }
     if (prims) {
-        CUDA_TRY(h, cudaMemcpy(tmp.data(), h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, sizeof(double4) * hc.nc,
-                               cudaMemcpyDeviceToHost));
+        rc = copy_sync(h, tmp, h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, sizeof(double4) * hc.nc,
+                       cudaMemcpyDeviceToHost);
+        if (rc) return rc;
         for (int64_t j = 0; j < hc.nc; ++j) {
             int64_t i = hc.cell_perm[j];
             prims[cidx(hc.nc, i, 0)] = tmp[j].x; prims[cidx(hc.nc, i, 1)] = tmp[j].y;
@@ -783,7 +822,8 @@ int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, 
         }
     }
     if (node_prims) {
-        CUDA_TRY(h, cudaMemcpy(tmp.data(), h->s.nodeP + hc.node_off, sizeof(double4) * hc.nn, cudaMemcpyDeviceToHost));
+        rc = copy_sync(h, tmp, h->s.nodeP + hc.node_off, sizeof(double4) * hc.nn, cudaMemcpyDeviceToHost);
+        if (rc) return rc;
         for (int64_t j = 0; j < hc.nn; ++j) {
             int64_t J = hc.node_perm[j];
             node_prims[cidx(hc.nn, J, 0)] = tmp[j].x; node_prims[cidx(hc.nn, J, 1)] = tmp[j].y;
@@ -831,6 +871,7 @@ int gd2d_destroy(gd2d_handle *h) {
     cudaStreamSynchronize(h->stream);
     drop_graph(h);
     for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
+    if (h->pinned) cudaFreeHost(h->pinned);
     h->buf.free_all();
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
