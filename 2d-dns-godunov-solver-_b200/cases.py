@@ -39,7 +39,7 @@ def square_inviscid(n_nodes: int = 101, seed: int = 1, flux: str = "ausm", limit
     AUSM+ / MUSCL / Minmod, CFL 0.5."""
     mesh = meshmod.unit_square_mesh(n_nodes, jitter=0.1, seed=seed)
     g = AIR["Gamma"]
-    cfg = {"thermo": dict(AIR), "flux": flux, "limiter": limiter, "viscosity": "none", "dt_mode": 1,
+    cfg = {"thermo": dict(AIR), "flux": flux, "limiter": limiter, "viscosity": "none", "dt_mode": 2,
            "CFL": 0.5, "beta": 1.0, "ksi": 1.0e-12, "init_nodes": 0,
            "bc": [{"tag": -1, "kind": "inflow", "rho": 1.0, "u": 2.0, "v": 0.0, "p": 1.0 / g},
                   {"tag": -2, "kind": "outflow"}, {"tag": -3, "kind": "slip"}]}
@@ -73,7 +73,7 @@ def cylinder_case(n_nodes: int = 1025, mach: float = 3.5, re_d: float = 1.0e4, r
     mu_inf = CYL_RHO * u_inf * D / re_d
     cfg = {"thermo": th, "flux": flux, "limiter": limiter,
            "viscosity": "sutherland" if viscous else "none", "art_viscosity": int(art_viscosity and viscous),
-           "mu_ref": mu_inf, "T_ref": T_inf, "Pr": 0.72, "venkat_K": 5.0, "dt_mode": 1, "CFL": cfl,
+           "mu_ref": mu_inf, "T_ref": T_inf, "Pr": 0.72, "venkat_K": 5.0, "dt_mode": 2, "CFL": cfl,
            "beta": 1.0, "ksi": 1.0e-12, "init_nodes": 0,
            "bc": [{"tag": -1, "kind": "inflow", "rho": CYL_RHO, "u": u_inf, "v": 0.0, "p": CYL_P},
                   {"tag": -2, "kind": "outflow"},
@@ -94,7 +94,7 @@ def tgv_case(n_nodes: int, mach: float, re: float, flux: str = "ausm", limiter: 
     p0 = 1.0 / g
     mu = 1.0 * U0 * 1.0 / re
     cfg = {"thermo": th, "flux": flux, "limiter": limiter, "viscosity": "constant", "art_viscosity": 0,
-           "mu_ref": mu, "T_ref": 1.0, "Pr": 0.72, "dt_mode": 1, "CFL": cfl, "beta": 1.0, "ksi": 1.0e-12,
+           "mu_ref": mu, "T_ref": 1.0, "Pr": 0.72, "dt_mode": 2, "CFL": cfl, "beta": 1.0, "ksi": 1.0e-12,
            "init_nodes": 0, "bc": []}
     x, y = mesh.cell_mid_points[:, 0], mesh.cell_mid_points[:, 1]
     u = U0 * np.sin(x) * np.cos(y)

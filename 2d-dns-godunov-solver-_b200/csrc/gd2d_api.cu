@@ -432,6 +432,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     for (int64_t g = 0; g < Nc; ++g) nbr[g] = make_int4(kAbsent, kAbsent, kAbsent, kAbsent);
     for (int64_t g = 0; g < Nc; ++g) { dn[g] = make_int4(0, 0, 0, 0); up[g] = make_int4(0, 0, 0, 0); }
     std::vector<int32_t> tile_case(ntiles, 0);
+    std::vector<int32_t> node_case(Nn, 0);
     h->hcases.resize(n_cases);
     for (int c = 0; c < n_cases; ++c) {
         const gd2d_mesh_view &mv = meshes[c];
@@ -503,6 +504,8 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         d.tile_begin = hc.cell_off / block;
         d.tile_end = (hc.cell_off + hc.nc_pad) / block;
         for (int64_t t = d.tile_begin; t < d.tile_end; ++t) tile_case[t] = c;
+        const int64_t node_end = (c + 1 < n_cases) ? h->cases[c + 1].node_off : Nn;
+        for (int64_t j = hc.node_off; j < node_end; ++j) node_case[j] = c;
         h->hcases[c] = d;
     }
     h->tile_case_h = tile_case;
@@ -517,7 +520,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     int2 *d_c2n;
     double *d_nx, *d_ny, *d_len, *d_rarea, *d_area, *d_hx, *d_charlen, *d_xn = nullptr, *d_yn = nullptr, *d_wt = nullptr;
     double2 *d_mid = nullptr;
-    int32_t *d_cl, *d_tc;
+    int32_t *d_cl, *d_tc, *d_nc = nullptr;
     DevCase *d_cases;
     auto bail = [&](int rc) { h->buf.free_all(); if (h->own_stream) cudaStreamDestroy(h->stream); g_setup_error = h->err; delete h; return rc; };
 #define ALLOC(ptr, n)                                                                              \
@@ -550,10 +553,12 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     ALLOC(d_cl, (size_t)W * Nn); UPLOAD(d_cl, cl);
     if (!unit) { ALLOC(d_wt, (size_t)W * Nn); UPLOAD(d_wt, wt); }
     ALLOC(d_tc, ntiles); UPLOAD(d_tc, tile_case);
+    if (h->visc) { ALLOC(d_nc, Nn); UPLOAD(d_nc, node_case); }
     ALLOC(d_cases, n_cases); UPLOAD(d_cases, h->hcases);
     m.nbr = d_nbr; m.dn = d_dn; m.up = d_up; m.dn2 = d_dn2; m.up2 = d_up2; m.c2n = d_c2n;
     m.nx = d_nx; m.ny = d_ny; m.len = d_len; m.rarea = d_rarea; m.area = d_area; m.hx = d_hx; m.charlen = d_charlen;
-    m.mid = d_mid; m.xnode = d_xn; m.ynode = d_yn; m.cl = d_cl; m.wt = d_wt; m.tile_case = d_tc; m.cases = d_cases;
+    m.mid = d_mid; m.xnode = d_xn; m.ynode = d_yn; m.cl = d_cl; m.wt = d_wt; m.tile_case = d_tc; m.node_case = d_nc;
+    m.cases = d_cases;
 
     s.ring_len = 1024;
     ALLOC(s.U, Nc);
@@ -684,9 +689,9 @@ static int capture_graph(gd2d_handle *h, int steps, bool timing) {
     CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < steps; ++k) {
         if (h->visc) launch_visc_grad_f64(h->m, h->s, h->lc, h->stream);
-        if (timing) cudaEventRecord(h->ev[2 * k], h->stream);
+        if (timing) cudaEventRecordWithFlags(h->ev[2 * k], h->stream, cudaEventRecordExternal);
         launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream);
-        if (timing) cudaEventRecord(h->ev[2 * k + 1], h->stream);
+        if (timing) cudaEventRecordWithFlags(h->ev[2 * k + 1], h->stream, cudaEventRecordExternal);
         launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream);
     }
     CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
@@ -747,6 +752,7 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
                     ++cell_samples;
                 }
             }
+            (void)cudaGetLastError();  // a failed timing query must not surface at the next launch
         }
         // history
         // the chunk's ring rows (the ring is [ring_len][ncases]; rows wrap)

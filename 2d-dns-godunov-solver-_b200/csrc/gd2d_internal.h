@@ -91,6 +91,7 @@ struct DevMesh {
     const int32_t *cl;                   // [cluster_w][Nn], -1 = empty
     const double *wt;                    // [cluster_w][Nn] (NULL if unit weights)
     const int32_t *tile_case;            // [ntiles]
+    const int32_t *node_case;            // [Nn] (viscous only)
     const DevCase *cases;
 };
 

@@ -178,12 +178,14 @@ __device__ __forceinline__ void face_flux(const DevMesh &m, const DevCase &P, co
     }
     double UpL[4], UpR[4];
     if (P.limiter == LIM_VENKAT) {
+        // eps^2 = (K*HX)^3 times the face's (uL^2 + uR^2)/2 of each variable
         double KL = P.venkat_K * hx_own, KR = P.venkat_K * hxR;
         double e2L = KL * KL * KL, e2R = KR * KR * KR;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            UpL[v] = uL[v] + 0.5 * lim_venkat(uL[v] - uDn[v], uR[v] - uL[v], e2L);
-            UpR[v] = uR[v] + 0.5 * lim_venkat(uR[v] - uUp[v], uL[v] - uR[v], e2R);
+            const double sc = 0.5 * (uL[v] * uL[v] + uR[v] * uR[v]);
+            UpL[v] = uL[v] + 0.5 * lim_venkat(uL[v] - uDn[v], uR[v] - uL[v], e2L * sc);
+            UpR[v] = uR[v] + 0.5 * lim_venkat(uR[v] - uUp[v], uL[v] - uR[v], e2R * sc);
         }
     } else {
         const int lk = P.limiter;
@@ -251,10 +253,11 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
                 if (tmp > 0.0) mart = 0.5 * me.x * HX / sqrt(2.0) * HX / sqrt(2.0) * sqrt(tmp) * 1.0e-5;
             }
         }
+        // laplacians of u, v and phi = |u|^2/2 + (gamma/Pr) e
         const double mue = mu + (P.art_visc ? mart : 0.0);
         diff[1] = mue * lap[0];
         diff[2] = mue * lap[1];
-        diff[3] = mue * P.gamma_over_Pr * lap[2];
+        diff[3] = mue * lap[2];
     }
 }
 
@@ -349,6 +352,14 @@ __global__ void __launch_bounds__(256) k_node_avg(const DevMesh m, const DevStat
     const double4 *__restrict__ src = s.prim + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
     const int W = m.cluster_w;
     for (int64_t J = n0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < n1; J += (int64_t)gridDim.x * blockDim.x) {
+        bool prim_form = false;
+        double gop = 0.0, gam = 0.0;
+        if (VISC) {
+            const DevCase &P = m.cases[m.node_case[J]];
+            prim_form = P.visc_model != VISC_REFERENCE;
+            gop = P.gamma_over_Pr;
+            gam = P.gamma;
+        }
         double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, det = 0.0;
         double c0 = 0.0, c1 = 0.0, c2 = 0.0;
         int cnt = 0;
@@ -360,8 +371,14 @@ __global__ void __launch_bounds__(256) k_node_avg(const DevMesh m, const DevStat
                 a0 = a0 + p.x * w; a1 = a1 + p.y * w; a2 = a2 + p.z * w; a3 = a3 + p.w * w;
                 det = det + w;
                 if (VISC) {
-                    const double4 u = s.U[c];
-                    c0 = c0 + u.y; c1 = c1 + u.z; c2 = c2 + u.w;
+                    if (prim_form) {
+                        // u, v, phi = |u|^2/2 + (gamma/Pr) p / ((gamma-1) rho)
+                        const double ph = 0.5 * (p.y * p.y + p.z * p.z) + gop * (p.w / ((gam - 1.0) * p.x));
+                        c0 = c0 + p.y; c1 = c1 + p.z; c2 = c2 + ph;
+                    } else {
+                        const double4 u = s.U[c];
+                        c0 = c0 + u.y; c1 = c1 + u.z; c2 = c2 + u.w;
+                    }
                     ++cnt;
                 }
             }

@@ -320,6 +320,29 @@ def structured_mesh(nx_nodes: int, ny_nodes: int, x0: float, x1: float, y0: floa
         cy = np.where(np.arange(4)[None, :] < nper[:, None], vy, 0.0).sum(1) / nper
         keep = ~np.asarray(remove(cx, cy), dtype=bool)
         ids, vx, vy, nper = ids[keep], vx[keep], vy[keep], nper[keep]
+        # Drop, repeatedly, cells left with two or more faces on the cut
+        # boundary (notches of the staircase with a single neighbour).
+        while True:
+            nfc = nper.max()
+            k = np.arange(nfc)
+            nxt = np.where(nper[:, None] == 4, (k[None, :] + 1) % 4, np.array([1, 2, 0, 0])[None, :nfc])
+            live = k[None, :] < nper[:, None]
+            a = ids[:, :nfc].astype(np.int64)
+            b = ids[np.arange(len(ids))[:, None], nxt].astype(np.int64)
+            key = np.minimum(a, b) * (node_x.shape[0] + 1) + np.maximum(a, b)
+            kl = key[live]
+            uniq, cnt = np.unique(kl, return_counts=True)
+            single = np.zeros(key.shape, dtype=bool)
+            single[live] = np.isin(kl, uniq[cnt == 1])
+            ax_, ay_ = vx[:, :nfc], vy[:, :nfc]
+            bx_, by_ = vx[np.arange(len(ids))[:, None], nxt], vy[np.arange(len(ids))[:, None], nxt]
+            outer = (((ax_ == x0) & (bx_ == x0)) | ((ax_ == x1) & (bx_ == x1)) |
+                     ((ay_ == y0) & (by_ == y0)) | ((ay_ == y1) & (by_ == y1)))
+            cut = (single & ~outer).sum(axis=1)
+            drop = cut >= 2
+            if not drop.any():
+                break
+            ids, vx, vy, nper = ids[~drop], vx[~drop], vy[~drop], nper[~drop]
         used = np.zeros(node_x.shape[0], dtype=bool)
         used[ids[ids >= 0]] = True
         remap = np.full(node_x.shape[0], -1, dtype=np.int64)

@@ -512,12 +512,15 @@ static void interface_flux(const orc_state *s, int64_t i, int k, const double *u
     double UpLeft[4], UpRight[4];
     if (s->p.limiter == ORC_LIM_VENKAT) {
         /* Extension: each side's reconstruction evaluated in its own
-         * (outer, central) roles so both cells of a face build the same state. */
+         * (outer, central) roles so both cells of a face build the same
+         * state; eps^2 = (K*HX)^3 scaled by the face's squared magnitude
+         * of the variable, (uL^2 + uR^2)/2, so that it is dimensionless. */
         double KL = s->p.venkat_K * s->m.HX[i], KR = s->p.venkat_K * hxR;
         double e2L = KL * KL * KL, e2R = KR * KR * KR;
         for (int v = 0; v < 4; ++v) {
-            UpLeft[v] = uLeftp[v] + 0.5 * orc_venkat(uLeftp[v] - uDownp[v], uRightp[v] - uLeftp[v], e2L);
-            UpRight[v] = uRightp[v] + 0.5 * orc_venkat(uRightp[v] - uUpp[v], uLeftp[v] - uRightp[v], e2R);
+            double sc = 0.5 * (uLeftp[v] * uLeftp[v] + uRightp[v] * uRightp[v]);
+            UpLeft[v] = uLeftp[v] + 0.5 * orc_venkat(uLeftp[v] - uDownp[v], uRightp[v] - uLeftp[v], e2L * sc);
+            UpRight[v] = uRightp[v] + 0.5 * orc_venkat(uRightp[v] - uUpp[v], uLeftp[v] - uRightp[v], e2R * sc);
         }
     } else {
         for (int v = 0; v < 4; ++v) {
@@ -774,15 +777,17 @@ static void diff_combine_range(orc_state *s, int64_t b, int64_t e, void *vctx) {
             IDX(s->UConsDiffCells, n, i, 3) = mu * orc_air_conductivity(T) * le;
         } else {
             /* Extension: mu(T) Sutherland scaled to mu_ref at T_ref (or a
-             * constant mu_ref), plus artificial viscosity; energy diffusivity
-             * k/cv = mu*gamma/Pr in the same Laplacian-of-conservatives form. */
+             * constant mu_ref), plus artificial viscosity, applied to the
+             * Laplacians of u, v and phi = |u|^2/2 + (gamma/Pr) e:
+             * div(tau) ~ mu lap(u), div(tau.u) + div(k grad T) ~
+             * mu lap(|u|^2/2) + (mu cp/Pr) lap(T). */
             double mu = (p->viscosity == ORC_VISC_SUTHERLAND)
                             ? p->mu_ref * (orc_sutherland(T) / s->suth_ref)
                             : p->mu_ref;
             double mue = mu + (p->art_viscosity ? s->muArt[i] : 0.0);
             IDX(s->UConsDiffCells, n, i, 1) = mue * lu;
             IDX(s->UConsDiffCells, n, i, 2) = mue * lv;
-            IDX(s->UConsDiffCells, n, i, 3) = mue * s->gamma_over_Pr * le;
+            IDX(s->UConsDiffCells, n, i, 3) = mue * le;
         }
     }
 }
@@ -795,10 +800,24 @@ typedef struct { int var; } lap_ctx;
 void orc_calc_diff_term(orc_state *s) {
     int64_t n = s->m.nCells;
     double *dummy = (double *)malloc(sizeof(double) * (size_t)n);
+    double *prim3 = NULL;
+    if (s->p.viscosity != ORC_VISC_REFERENCE) {
+        /* Extension models diffuse primitive quantities: u, v and
+         * phi = |u|^2/2 + (gamma/Pr) e, e = p / ((gamma-1) rho). */
+        const double G = s->p.Gamma;
+        prim3 = (double *)malloc(sizeof(double) * 3 * (size_t)n);
+        for (int64_t i = 0; i < n; ++i) {
+            double r = s->densityCells[i], u = s->UxCells[i], v = s->UyCells[i], pp = s->pressureCells[i];
+            prim3[i] = u;
+            prim3[n + i] = v;
+            prim3[2 * n + i] = 0.5 * (u * u + v * v) + s->gamma_over_Pr * (pp / ((G - 1.0) * r));
+        }
+    }
     for (int v = 0; v < 3; ++v) {
-        const double *field = s->UconsCellsOld + (int64_t)(v + 1) * n;
+        const double *field = prim3 ? prim3 + (int64_t)v * n : s->UconsCellsOld + (int64_t)(v + 1) * n;
         gg_gradient(s, field, s->g1x[v], s->g1y[v]);
     }
+    free(prim3);
     for (int v = 0; v < 3; ++v) {
         double *d2x = s->lap[v]; /* temporarily holds d/dy(gradX) */
         double *tmp = (double *)malloc(sizeof(double) * (size_t)n);
