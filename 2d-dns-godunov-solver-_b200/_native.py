@@ -49,9 +49,10 @@ class Params(C.Structure):
                 ("kGas", C.c_double), ("CFL", C.c_double), ("dt", C.c_double), ("beta", C.c_double),
                 ("ksi", C.c_double), ("venkat_K", C.c_double), ("mu_ref", C.c_double), ("T_ref", C.c_double),
                 ("Pr", C.c_double), ("tgv_U0", C.c_double), ("tgv_P0", C.c_double), ("tgv_L", C.c_double),
-                ("tgv_mu", C.c_double), ("start_time", C.c_double), ("flux", C.c_int32),
-                ("limiter", C.c_int32), ("viscosity", C.c_int32), ("art_viscosity", C.c_int32),
-                ("dt_mode", C.c_int32), ("init_nodes", C.c_int32), ("n_bc", C.c_int32), ("reserved0", C.c_int32),
+                ("tgv_mu", C.c_double), ("start_time", C.c_double), ("min_density", C.c_double),
+                ("max_density", C.c_double), ("flux", C.c_int32), ("limiter", C.c_int32),
+                ("viscosity", C.c_int32), ("art_viscosity", C.c_int32), ("dt_mode", C.c_int32),
+                ("init_nodes", C.c_int32), ("n_bc", C.c_int32), ("density_constrained", C.c_int32),
                 ("bc", BC * GD2D_MAX_BC)]
 
 

@@ -75,6 +75,10 @@ def cylinder_case(n_nodes: int = 1025, mach: float = 3.5, re_d: float = 1.0e4, r
            "viscosity": "sutherland" if viscous else "none", "art_viscosity": int(art_viscosity and viscous),
            "mu_ref": mu_inf, "T_ref": T_inf, "Pr": 0.72, "venkat_K": 5.0, "dt_mode": 2, "CFL": cfl,
            "beta": 1.0, "ksi": 1.0e-12, "init_nodes": 0,
+           # the reference's density constraint with its default bounds
+           # (setupSolver_step2d.jl:167-169): the base region behind the
+           # cylinder expands towards vacuum after the impulsive start
+           "densityConstrained": 1, "minDensityConstrained": 0.01, "maxDensityConstrained": 10.0,
            "bc": [{"tag": -1, "kind": "inflow", "rho": CYL_RHO, "u": u_inf, "v": 0.0, "p": CYL_P},
                   {"tag": -2, "kind": "outflow"},
                   {"tag": -4, "kind": "noslip_isothermal", "Tw": T_inf}]}

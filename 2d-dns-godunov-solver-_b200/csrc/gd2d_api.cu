@@ -260,6 +260,9 @@ DevCase make_devcase(const gd2d_params &p, double maxEdge) {
         d.bc_p[b] = p.bc[b].p;
         d.bc_Tw[b] = p.bc[b].Tw;
     }
+    d.rho_min = p.min_density;
+    d.rho_max = p.max_density;
+    d.density_constrained = p.density_constrained;
     d.dt_mode = p.dt_mode;
     d.visc_model = p.viscosity;
     d.art_visc = p.art_viscosity;

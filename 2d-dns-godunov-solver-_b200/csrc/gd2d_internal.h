@@ -44,9 +44,11 @@ struct DevCase {
     double gamma, R, CFL, dt_fixed, beta, ksi, venkat_K;
     double mu_ref, suth_ref, gamma_over_Pr, maxEdge;
     double tgv_U0, tgv_P0, tgv_L, tgv_mu;
+    double rho_min, rho_max;          // densityConstrained clamp
     double bc_rho[kMaxBC], bc_u[kMaxBC], bc_v[kMaxBC], bc_p[kMaxBC], bc_Tw[kMaxBC];
     int32_t bc_kind[kMaxBC];
     int32_t dt_mode, visc_model, art_visc, limiter;
+    int32_t density_constrained, pad_;
     int64_t cell_begin, cell_end;   // padded global cell range [begin, end)
     int64_t tile_begin, tile_end;   // tiles of the cell kernel
 };

@@ -310,6 +310,10 @@ __global__ void __launch_bounds__(256) k_cell_step(const DevMesh m, const DevSta
             double Un[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) Un[v] = (Uo[v] - F[v] * P.beta * dt * rarea + P.beta * dt * diff[v]);
+            if (P.density_constrained == 1) {  // evaluate2d.jl:63-77
+                if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
+                if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
+            }
             s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
             // updateVariablesSA, evaluate2d.jl:87-104
             const double rho = Un[0];

@@ -59,6 +59,9 @@ def make_params(cfg: Dict) -> N.Params:
     p.tgv_U0, p.tgv_P0 = tgv.get("U0", 40.0), tgv.get("P0", 100000.0)
     p.tgv_L, p.tgv_mu = tgv.get("L", 1.0), tgv.get("mu", 1.0e-2)
     p.start_time = cfg.get("start_time", 0.0)
+    p.density_constrained = int(cfg.get("densityConstrained", 0))
+    p.min_density = cfg.get("minDensityConstrained", 0.01)
+    p.max_density = cfg.get("maxDensityConstrained", 10.0)
     p.flux = N.FLUX[cfg.get("flux", "ausm")]
     p.limiter = N.LIMITER[cfg.get("limiter", "minmod")]
     p.viscosity = N.VISC[cfg.get("viscosity", "none")]

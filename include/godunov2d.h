@@ -103,11 +103,12 @@ typedef struct gd2d_params {
     double Pr;
     double tgv_U0, tgv_P0, tgv_L, tgv_mu;  /* computeTGV2d (initfields_TGV2d.jl:9-27) */
     double start_time;
+    double min_density, max_density;  /* minDensityConstrained / maxDensityConstrained */
     int32_t flux, limiter, viscosity, art_viscosity;
     int32_t dt_mode;
     int32_t init_nodes;     /* 0: node primitives zero in step 1, as the reference */
     int32_t n_bc;
-    int32_t reserved0;
+    int32_t density_constrained;  /* densityConstrained: clamp the new density (evaluate2d.jl:63-77) */
     gd2d_bc bc[GD2D_MAX_BC];
 } gd2d_params;
 

@@ -76,11 +76,14 @@ typedef struct {
     double T_ref;        /* temperature where mu = mu_ref (Sutherland) */
     double Pr;
     double tgv_U0, tgv_P0, tgv_L, tgv_mu;  /* computeTGV2d constants */
+    double minDensityConstrained, maxDensityConstrained;  /* CONTROLS, primeObjects.jl:241-242 */
     int32_t flux, limiter, viscosity, art_viscosity;
     int32_t dt_mode;     /* 0: fixed dt, 1: dt = CFL-based tau */
     int32_t init_nodes;  /* 0: node primitives zero at step 1 (reference) */
     int32_t nthreads;
     int32_t n_bc;
+    int32_t densityConstrained;  /* CONTROLS flag, primeObjects.jl:240 */
+    int32_t pad2_;
     orc_bc bc[ORC_MAX_BC];
 } orc_params;
 
@@ -577,6 +580,14 @@ static void update_range(orc_state *s, int64_t b, int64_t e, void *vctx) {
     int64_t n = s->m.nCells;
     double G = s->p.Gamma;
     for (int64_t i = b; i < e; ++i) {
+        if (s->p.densityConstrained == 1) {
+            /* evaluate2d.jl:63-77 (the reference indexes an array that is
+             * out of scope there; the clamp acts on Unew as intended). */
+            if (IDX(s->UconsCellsNew, n, i, 0) >= s->p.maxDensityConstrained)
+                IDX(s->UconsCellsNew, n, i, 0) = s->p.maxDensityConstrained;
+            if (IDX(s->UconsCellsNew, n, i, 0) <= s->p.minDensityConstrained)
+                IDX(s->UconsCellsNew, n, i, 0) = s->p.minDensityConstrained;
+        }
         double U1 = IDX(s->UconsCellsNew, n, i, 0), U2 = IDX(s->UconsCellsNew, n, i, 1);
         double U3 = IDX(s->UconsCellsNew, n, i, 2), U4 = IDX(s->UconsCellsNew, n, i, 3);
         s->densityCells[i] = U1;

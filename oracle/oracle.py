@@ -50,9 +50,11 @@ class OrcParams(C.Structure):
                 ("kGas", C.c_double), ("CFL", C.c_double), ("dt", C.c_double), ("beta", C.c_double),
                 ("ksi", C.c_double), ("venkat_K", C.c_double), ("mu_ref", C.c_double), ("T_ref", C.c_double),
                 ("Pr", C.c_double), ("tgv_U0", C.c_double), ("tgv_P0", C.c_double), ("tgv_L", C.c_double),
-                ("tgv_mu", C.c_double), ("flux", C.c_int32), ("limiter", C.c_int32), ("viscosity", C.c_int32),
-                ("art_viscosity", C.c_int32), ("dt_mode", C.c_int32), ("init_nodes", C.c_int32),
-                ("nthreads", C.c_int32), ("n_bc", C.c_int32), ("bc", OrcBC * 8)]
+                ("tgv_mu", C.c_double), ("minDensityConstrained", C.c_double),
+                ("maxDensityConstrained", C.c_double), ("flux", C.c_int32), ("limiter", C.c_int32),
+                ("viscosity", C.c_int32), ("art_viscosity", C.c_int32), ("dt_mode", C.c_int32),
+                ("init_nodes", C.c_int32), ("nthreads", C.c_int32), ("n_bc", C.c_int32),
+                ("densityConstrained", C.c_int32), ("pad2_", C.c_int32), ("bc", OrcBC * 8)]
 
 
 class OrcStats(C.Structure):
@@ -145,6 +147,9 @@ def make_params(cfg) -> OrcParams:
     tgv = cfg.get("tgv", {})
     p.tgv_U0, p.tgv_P0, p.tgv_L, p.tgv_mu = (tgv.get("U0", 40.0), tgv.get("P0", 100000.0), tgv.get("L", 1.0),
                                               tgv.get("mu", 1.0e-2))
+    p.densityConstrained = int(cfg.get("densityConstrained", 0))
+    p.minDensityConstrained = cfg.get("minDensityConstrained", 0.01)
+    p.maxDensityConstrained = cfg.get("maxDensityConstrained", 10.0)
     p.flux = FLUX[cfg.get("flux", "ausm")]
     p.limiter = LIMITER[cfg.get("limiter", "minmod")]
     p.viscosity = VISC[cfg.get("viscosity", "none")]
