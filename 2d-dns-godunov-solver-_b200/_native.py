@@ -26,7 +26,8 @@ LOOP = {"cell": 0, "face": 1}
 
 EXPORTS = ("gd2d_abi_version", "gd2d_last_error", "gd2d_setup", "gd2d_set_state", "gd2d_set_conservative",
            "gd2d_propagate", "gd2d_get_history", "gd2d_get_state", "gd2d_calc_one_stage", "gd2d_update_variables",
-           "gd2d_cells_to_nodes", "gd2d_calc_diff_term", "gd2d_autotune", "gd2d_last_timing", "gd2d_destroy")
+           "gd2d_cells_to_nodes", "gd2d_calc_diff_term", "gd2d_autotune", "gd2d_last_timing", "gd2d_destroy",
+           "gd2d_update_variables_noalloc")
 
 
 class MeshView(C.Structure):
@@ -109,6 +110,7 @@ def load(path: str = LIB_PATH):
     L.gd2d_autotune.argtypes = [vp, i32, C.POINTER(Launch)]
     L.gd2d_last_timing.argtypes = [vp, dp, dp, C.POINTER(i64)]
     L.gd2d_destroy.argtypes = [vp]
+    L.gd2d_update_variables_noalloc.argtypes = [vp, vp, vp, i64, C.c_double, vp, vp]
     for name in EXPORTS:
         if name not in ("gd2d_last_error",):
             getattr(L, name).restype = C.c_int

@@ -284,6 +284,13 @@ int gd2d_abi_version(void) { return GD2D_ABI_VERSION; }
 
 const char *gd2d_last_error(const gd2d_handle *h) { return h ? h->err.c_str() : g_setup_error.c_str(); }
 
+}  // extern "C"
+
+// Error message of handle-less entry points, read back by gd2d_last_error(NULL).
+void gd2d::set_handleless_error(const char *msg) { g_setup_error = msg; }
+
+extern "C" {
+
 int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes, const gd2d_params *params,
                const gd2d_launch *launch) {
     if (!out) return fail(nullptr, GD2D_ERR_ARG, "out is NULL");

@@ -120,6 +120,9 @@ struct LaunchCfg {
     int grid;        // persistent grid size
 };
 
+// Message reported by gd2d_last_error(NULL) for calls without a handle.
+void set_handleless_error(const char *msg);
+
 // Launchers implemented in kernels_f64.cu.
 cudaError_t launch_cell_step_f64(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
                                  const LaunchCfg &lc, cudaStream_t st);

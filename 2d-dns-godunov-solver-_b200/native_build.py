@@ -26,6 +26,7 @@ UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_mixed.cu", []),
     ("gd2d_api.cu", []),
+    ("gd2d_noalloc.cu", ["-fmad=false"]),
 ]
 
 

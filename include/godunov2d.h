@@ -202,6 +202,22 @@ int gd2d_last_timing(gd2d_handle *h, double *total_ms, double *cell_kernel_ms, i
 
 int gd2d_destroy(gd2d_handle *h);
 
+/* updateVariablesSA + residuals on caller-owned DEVICE arrays, allocating
+ * nothing.  No counterpart in the reference: it exists for callers that
+ * cannot let a library allocate -- memory owned by their own pool (Julia's
+ * CUDA.jl, a caching allocator) or an allocation-free step loop (cudaMalloc
+ * synchronises the device and is not allowed during stream capture).
+ * d_unew, d_uold, d_prims: [n_cells x 4] column-major device arrays (d_uold is
+ * overwritten with d_unew, d_prims receives rho, u, v, p); d_stats: 6 device
+ * doubles = sum of (Unew-Uold)^2 per variable, max VMAX, non-finite flag.
+ * The only scratch is a fixed 4 MiB array inside the library (one per GPU,
+ * held until exit), so n_cells is limited to 16,777,216 (larger: GD2D_ERR_ARG).
+ * The first call on a device looks that array up and should come before any
+ * stream capture; calls that overlap on the GPU share the array and race.
+ * Runs on `stream` (NULL: the legacy default stream). */
+int gd2d_update_variables_noalloc(const double *d_unew, double *d_uold, double *d_prims, int64_t n_cells,
+                                  double gamma, double *d_stats, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
