@@ -338,6 +338,11 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     h->lc.block = block;
     h->lc.node_block = h->launch.node_block ? h->launch.node_block : 256;
     h->lc.persistent = h->launch.persistent;
+    h->lc.min_blocks = h->launch.min_blocks ? h->launch.min_blocks : 2;
+    if (h->lc.min_blocks < 2 || h->lc.min_blocks > 4) {
+        delete h;
+        return fail(nullptr, GD2D_ERR_ARG, "min_blocks must be 2, 3 or 4");
+    }
     h->graph_steps = h->launch.graph_steps > 0 ? h->launch.graph_steps : 32;
     h->flux = params[0].flux;
     h->visc = params[0].viscosity != GD2D_VISC_NONE;
@@ -585,9 +590,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     {
         int dev_sms = 148;
         cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
-        int per_sm = 0;
-        h->lc.grid = dev_sms * 8;
-        (void)per_sm;
+        h->lc.grid = dev_sms * h->lc.min_blocks * (256 / block);
     }
     h->history.assign(n_cases, {});
     h->cs_host.assign(n_cases, CaseState{});

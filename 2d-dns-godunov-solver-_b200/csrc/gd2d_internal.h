@@ -118,6 +118,7 @@ struct LaunchCfg {
     int node_block;
     int persistent;
     int grid;        // persistent grid size
+    int min_blocks;  // register budget of the cell kernel: blocks per SM (2, 3, 4)
 };
 
 // Message reported by gd2d_last_error(NULL) for calls without a handle.

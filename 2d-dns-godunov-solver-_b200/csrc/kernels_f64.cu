@@ -18,7 +18,10 @@ int grid_for(int64_t work, int block) {
 template <int FLUX, bool VISC, bool QUAD>
 cudaError_t cell_step(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
     int grid = lc.persistent ? lc.grid : (int)m.ntiles;
-    k_cell_step<FLUX, VISC, QUAD><<<grid, lc.block, 0, st>>>(m, s);
+    // register budget chosen by the launch configuration (blocks per SM)
+    if (lc.min_blocks >= 4) k_cell_step<FLUX, VISC, QUAD, 4><<<grid, lc.block, 0, st>>>(m, s);
+    else if (lc.min_blocks == 3) k_cell_step<FLUX, VISC, QUAD, 3><<<grid, lc.block, 0, st>>>(m, s);
+    else k_cell_step<FLUX, VISC, QUAD, 2><<<grid, lc.block, 0, st>>>(m, s);
     return cudaGetLastError();
 }
 

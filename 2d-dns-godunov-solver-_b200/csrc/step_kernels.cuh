@@ -263,8 +263,8 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
 
 // ---------------------------------------------------- fused cell kernel
 
-template <int FLUX, bool VISC, bool QUAD>
-__global__ void __launch_bounds__(256) k_cell_step(const DevMesh m, const DevState s) {
+template <int FLUX, bool VISC, bool QUAD, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const DevState s) {
     __shared__ Part sh[8];
     const int par = *s.parity;
     const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;

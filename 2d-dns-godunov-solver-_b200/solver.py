@@ -81,12 +81,13 @@ def make_params(cfg: Dict) -> N.Params:
 
 
 def make_launch(precision="f64", order="hilbert", loop="cell", block=0, node_block=0, persistent=0,
-                graph_steps=0, stream=None) -> N.Launch:
+                graph_steps=0, stream=None, min_blocks=0) -> N.Launch:
     l = N.Launch()
     l.precision = N.PRECISION[precision] if isinstance(precision, str) else int(precision)
     l.order = N.ORDER[order] if isinstance(order, str) else int(order)
     l.loop = N.LOOP[loop] if isinstance(loop, str) else int(loop)
     l.block, l.node_block, l.persistent, l.graph_steps = block, node_block, persistent, graph_steps
+    l.min_blocks = min_blocks
     l.stream = stream
     return l
 
