@@ -81,6 +81,9 @@ struct gd2d_handle {
     int64_t last_launches = 0;
     double4 *pinned = nullptr;  // page-locked staging for state uploads and downloads
     size_t pinned_count = 0;
+    // single-function entry points
+    double4 *split_unew = nullptr, *split_flux = nullptr, *split_delta = nullptr, *split_diff = nullptr;
+    bool split_stage_done = false, split_diff_valid = false;
     std::vector<CaseState> cs_host;
     std::string err;
 };
@@ -326,10 +329,11 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     gd2d_handle *h = new gd2d_handle();
     h->ncases = n_cases;
     if (launch) h->launch = *launch;
-    if (h->launch.precision != GD2D_PREC_F64) {
+    if (h->launch.precision != GD2D_PREC_F64 && h->launch.precision != GD2D_PREC_MIXED) {
         delete h;
-        return fail(nullptr, GD2D_ERR_ARG, "precision %d not available in this build", launch->precision);
+        return fail(nullptr, GD2D_ERR_ARG, "unknown precision %d", launch->precision);
     }
+    h->mixed = h->launch.precision == GD2D_PREC_MIXED;
     int block = h->launch.block ? h->launch.block : 256;
     if (block != 128 && block != 256) {
         delete h;
@@ -338,7 +342,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     h->lc.block = block;
     h->lc.node_block = h->launch.node_block ? h->launch.node_block : 256;
     h->lc.persistent = h->launch.persistent;
-    h->lc.min_blocks = h->launch.min_blocks ? h->launch.min_blocks : 2;
+    h->lc.min_blocks = h->launch.min_blocks ? h->launch.min_blocks : 3;
     if (h->lc.min_blocks < 2 || h->lc.min_blocks > 4) {
         delete h;
         return fail(nullptr, GD2D_ERR_ARG, "min_blocks must be 2, 3 or 4");
@@ -553,13 +557,32 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     ALLOC(d_up, Nc); UPLOAD(d_up, up);
     if (h->quads) { ALLOC(d_dn2, Nc); UPLOAD(d_dn2, dn2); ALLOC(d_up2, Nc); UPLOAD(d_up2, up2); }
     ALLOC(d_c2n, (size_t)nfmax * Nc); UPLOAD(d_c2n, c2n);
-    ALLOC(d_nx, (size_t)nfmax * Nc); UPLOAD(d_nx, gnx);
-    ALLOC(d_ny, (size_t)nfmax * Nc); UPLOAD(d_ny, gny);
-    ALLOC(d_len, (size_t)nfmax * Nc); UPLOAD(d_len, glen);
-    ALLOC(d_rarea, Nc); UPLOAD(d_rarea, rarea);
-    ALLOC(d_area, Nc); UPLOAD(d_area, area);
-    ALLOC(d_hx, Nc); UPLOAD(d_hx, hx);
-    ALLOC(d_charlen, Nc); UPLOAD(d_charlen, charlen);
+    if (!h->mixed) {
+        ALLOC(d_nx, (size_t)nfmax * Nc); UPLOAD(d_nx, gnx);
+        ALLOC(d_ny, (size_t)nfmax * Nc); UPLOAD(d_ny, gny);
+        ALLOC(d_len, (size_t)nfmax * Nc); UPLOAD(d_len, glen);
+        ALLOC(d_rarea, Nc); UPLOAD(d_rarea, rarea);
+        ALLOC(d_area, Nc); UPLOAD(d_area, area);
+        ALLOC(d_hx, Nc); UPLOAD(d_hx, hx);
+        ALLOC(d_charlen, Nc); UPLOAD(d_charlen, charlen);
+    } else {
+        d_nx = d_ny = d_len = d_rarea = d_area = d_hx = d_charlen = nullptr;
+        auto to_f = [](const std::vector<double> &v) {
+            std::vector<float> f(v.size());
+            for (size_t i = 0; i < v.size(); ++i) f[i] = (float)v[i];
+            return f;
+        };
+        float *f_nx, *f_ny, *f_len, *f_rarea, *f_area, *f_hx, *f_charlen;
+        ALLOC(f_nx, (size_t)nfmax * Nc); UPLOAD(f_nx, to_f(gnx));
+        ALLOC(f_ny, (size_t)nfmax * Nc); UPLOAD(f_ny, to_f(gny));
+        ALLOC(f_len, (size_t)nfmax * Nc); UPLOAD(f_len, to_f(glen));
+        ALLOC(f_rarea, Nc); UPLOAD(f_rarea, to_f(rarea));
+        ALLOC(f_area, Nc); UPLOAD(f_area, to_f(area));
+        ALLOC(f_hx, Nc); UPLOAD(f_hx, to_f(hx));
+        ALLOC(f_charlen, Nc); UPLOAD(f_charlen, to_f(charlen));
+        m.nxf = f_nx; m.nyf = f_ny; m.lenf = f_len; m.rareaf = f_rarea; m.areaf = f_area; m.hxf = f_hx;
+        m.charlenf = f_charlen;
+    }
     if (h->tgv) {
         ALLOC(d_mid, Nc); UPLOAD(d_mid, mid);
         ALLOC(d_xn, Nn); UPLOAD(d_xn, xnode);
@@ -577,9 +600,15 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
 
     s.ring_len = 1024;
     ALLOC(s.U, Nc);
-    ALLOC(s.prim, 2 * Nc);
-    ALLOC(s.nodeP, Nn);
-    if (h->visc) { ALLOC(s.nodeC, Nn); ALLOC(s.g1, Nc); ALLOC(s.nodeG, Nn); }
+    if (!h->mixed) {
+        ALLOC(s.prim, 2 * Nc);
+        ALLOC(s.nodeP, Nn);
+        if (h->visc) { ALLOC(s.nodeC, Nn); ALLOC(s.g1, Nc); ALLOC(s.nodeG, Nn); }
+    } else {
+        ALLOC(s.primf, 2 * Nc);
+        ALLOC(s.nodePf, Nn);
+        if (h->visc) { ALLOC(s.nodeCf, Nn); ALLOC(s.g1f, Nc); ALLOC(s.nodeGf, Nn); }
+    }
     ALLOC(s.part, (size_t)ntiles * kPartials);
     ALLOC(s.cstate, n_cases);
     ALLOC(s.ring, (size_t)s.ring_len * n_cases);
@@ -642,17 +671,25 @@ static int init_case_from_pinned(gd2d_handle *h, int32_t icase, double t0, bool 
     int par = 0;
     int rc = copy_sync(h, &par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost);
     if (rc) return rc;
-    CUDA_TRY(h, cudaMemcpyAsync(h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, h->pinned, sizeof(double4) * hc.nc,
-                                cudaMemcpyHostToDevice, h->stream));
+    // FP64: the primitives go to the current buffer; mixed: to U, which the
+    // init kernel turns into conservatives while writing the FP32 primitives
+    double4 *dst = h->mixed ? h->s.U + hc.cell_off : h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off;
+    CUDA_TRY(h, cudaMemcpyAsync(dst, h->pinned, sizeof(double4) * hc.nc, cudaMemcpyHostToDevice, h->stream));
     CaseState &cs = h->cs_host[icase];
     cs = CaseState{};
     cs.t = t0;
     CUDA_TRY(h, cudaMemcpyAsync(h->s.cstate + icase, &cs, sizeof cs, cudaMemcpyHostToDevice, h->stream));
     // per-case init restricted to this case's tiles and nodes
     const DevCase &d = h->hcases[icase];
-    CUDA_TRY(h, launch_init_state_f64(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
-    CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off, hc.node_off + hc.nn,
-                                    h->lc, h->stream));
+    if (h->mixed) {
+        CUDA_TRY(h, launch_init_state_mixed(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
+        CUDA_TRY(h, launch_node_avg_mixed(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off,
+                                          hc.node_off + hc.nn, h->lc, h->stream));
+    } else {
+        CUDA_TRY(h, launch_init_state_f64(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
+        CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off,
+                                        hc.node_off + hc.nn, h->lc, h->stream));
+    }
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     hc.state_set = true;
     h->history[icase].clear();
@@ -692,6 +729,24 @@ int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, do
     return init_case_from_pinned(h, icase, flow_time, rebuild_nodes != 0);
 }
 
+// The kernels of one step on the handle's stream: [viscous gradient passes]
+// -> fused cell kernel (bracketed by the optional timing events) -> node pass.
+static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, cudaEvent_t after_cell) {
+    cudaError_t e = cudaSuccess;
+    if (h->visc) {
+        e = h->mixed ? launch_visc_grad_mixed(h->m, h->s, h->lc, h->stream)
+                     : launch_visc_grad_f64(h->m, h->s, h->lc, h->stream);
+        if (e != cudaSuccess) return e;
+    }
+    if (before_cell) cudaEventRecordWithFlags(before_cell, h->stream, cudaEventRecordExternal);
+    e = h->mixed ? launch_cell_step_mixed(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream)
+                 : launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream);
+    if (e != cudaSuccess) return e;
+    if (after_cell) cudaEventRecordWithFlags(after_cell, h->stream, cudaEventRecordExternal);
+    return h->mixed ? launch_node_avg_mixed(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream)
+                    : launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream);
+}
+
 static int capture_graph(gd2d_handle *h, int steps, bool timing) {
     drop_graph(h);
     if (timing) {
@@ -701,11 +756,7 @@ static int capture_graph(gd2d_handle *h, int steps, bool timing) {
     cudaGraph_t g;
     CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < steps; ++k) {
-        if (h->visc) launch_visc_grad_f64(h->m, h->s, h->lc, h->stream);
-        if (timing) cudaEventRecordWithFlags(h->ev[2 * k], h->stream, cudaEventRecordExternal);
-        launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream);
-        if (timing) cudaEventRecordWithFlags(h->ev[2 * k + 1], h->stream, cudaEventRecordExternal);
-        launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream);
+        launch_step_kernels(h, timing ? h->ev[2 * k] : nullptr, timing ? h->ev[2 * k + 1] : nullptr);
     }
     CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
@@ -747,9 +798,7 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
             }
         }
         for (; k < chunk; ++k) {
-            if (h->visc) CUDA_TRY(h, launch_visc_grad_f64(h->m, h->s, h->lc, h->stream));
-            CUDA_TRY(h, launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream));
-            CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream));
+            CUDA_TRY(h, launch_step_kernels(h, nullptr, nullptr));
             launches += h->visc ? 4 : 2;
         }
         CUDA_TRY(h, cudaEventRecord(h->ev_total[1], h->stream));
@@ -830,6 +879,29 @@ int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, 
             ucons[cidx(hc.nc, i, 2)] = tmp[j].z; ucons[cidx(hc.nc, i, 3)] = tmp[j].w;
         }
     }
+    if (prims && h->mixed) {
+        float4 *tf = reinterpret_cast<float4 *>(h->pinned);
+        rc = copy_sync(h, tf, h->s.primf + (int64_t)par * h->m.Nc + hc.cell_off, sizeof(float4) * hc.nc,
+                       cudaMemcpyDeviceToHost);
+        if (rc) return rc;
+        for (int64_t j = 0; j < hc.nc; ++j) {
+            int64_t i = hc.cell_perm[j];
+            prims[cidx(hc.nc, i, 0)] = tf[j].x; prims[cidx(hc.nc, i, 1)] = tf[j].y;
+            prims[cidx(hc.nc, i, 2)] = tf[j].z; prims[cidx(hc.nc, i, 3)] = tf[j].w;
+        }
+        prims = nullptr;
+    }
+    if (node_prims && h->mixed) {
+        float4 *tf = reinterpret_cast<float4 *>(h->pinned);
+        rc = copy_sync(h, tf, h->s.nodePf + hc.node_off, sizeof(float4) * hc.nn, cudaMemcpyDeviceToHost);
+        if (rc) return rc;
+        for (int64_t j = 0; j < hc.nn; ++j) {
+            int64_t J = hc.node_perm[j];
+            node_prims[cidx(hc.nn, J, 0)] = tf[j].x; node_prims[cidx(hc.nn, J, 1)] = tf[j].y;
+            node_prims[cidx(hc.nn, J, 2)] = tf[j].z; node_prims[cidx(hc.nn, J, 3)] = tf[j].w;
+        }
+        node_prims = nullptr;
+    }
     if (prims) {
         rc = copy_sync(h, tmp, h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, sizeof(double4) * hc.nc,
                        cudaMemcpyDeviceToHost);
@@ -852,24 +924,84 @@ int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, 
     return GD2D_OK;
 }
 
-int gd2d_calc_one_stage(gd2d_handle *h, int32_t icase, double, double, double, double *, double *) {
+// Buffers of the one-function-at-a-time entry points, allocated on first use.
+static int split_buffers(gd2d_handle *h) {
+    if (h->mixed) return fail(h, GD2D_ERR_STATE, "the single-function entry points run the FP64 path only");
+    if (!h->state_ready) return fail(h, GD2D_ERR_STATE, "gd2d_set_state must be called for every case first");
+    if (!h->split_unew) {
+        CUDA_TRY(h, h->buf.alloc(&h->split_unew, (size_t)h->m.Nc));
+        CUDA_TRY(h, h->buf.alloc(&h->split_flux, (size_t)h->m.Nc));
+        CUDA_TRY(h, h->buf.alloc(&h->split_delta, (size_t)h->m.Nc));
+        CUDA_TRY(h, h->buf.alloc(&h->split_diff, (size_t)h->m.Nc));
+        CUDA_TRY(h, cudaDeviceSynchronize());
+    }
+    return GD2D_OK;
+}
+
+// A per-cell double4 field of one case to an (nCells x 4) column-major host
+// matrix in reference order.
+static int download_cells(gd2d_handle *h, int32_t icase, const double4 *src, double *dst) {
+    if (!dst) return GD2D_OK;
+    HostCase &hc = h->cases[icase];
+    int rc = copy_sync(h, h->pinned, src + hc.cell_off, sizeof(double4) * hc.nc, cudaMemcpyDeviceToHost);
+    if (rc) return rc;
+    const double4 *t = h->pinned;
+    for (int64_t j = 0; j < hc.nc; ++j) {
+        int64_t i = hc.cell_perm[j];
+        dst[cidx(hc.nc, i, 0)] = t[j].x; dst[cidx(hc.nc, i, 1)] = t[j].y;
+        dst[cidx(hc.nc, i, 2)] = t[j].z; dst[cidx(hc.nc, i, 3)] = t[j].w;
+    }
+    return GD2D_OK;
+}
+
+int gd2d_calc_one_stage(gd2d_handle *h, int32_t icase, double beta, double dt, double flow_time, double *fluxes,
+                        double *unew) {
     int rc = ensure_case(h, icase);
     if (rc) return rc;
-    return fail(h, GD2D_ERR_STATE, "gd2d_calc_one_stage: not built yet");
+    if ((rc = split_buffers(h))) return rc;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, launch_stage_only_f64(h->m, h->s, h->flux, h->quads, beta, dt, flow_time,
+                                      h->split_diff_valid ? h->split_diff : nullptr, h->split_unew, h->split_flux,
+                                      h->lc, h->stream));
+    if ((rc = download_cells(h, icase, h->split_flux, fluxes))) return rc;
+    if ((rc = download_cells(h, icase, h->split_unew, unew))) return rc;
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    h->split_stage_done = true;
+    return GD2D_OK;
 }
-int gd2d_update_variables(gd2d_handle *h, int32_t icase, double *) {
+
+int gd2d_update_variables(gd2d_handle *h, int32_t icase, double *delta) {
     int rc = ensure_case(h, icase);
     if (rc) return rc;
-    return fail(h, GD2D_ERR_STATE, "gd2d_update_variables: not built yet");
+    if ((rc = split_buffers(h))) return rc;
+    if (!h->split_stage_done) return fail(h, GD2D_ERR_STATE, "gd2d_calc_one_stage must run first");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, launch_update_only_f64(h->m, h->s, h->split_unew, h->split_delta, h->lc, h->stream));
+    h->split_stage_done = false;
+    h->split_diff_valid = false;
+    return download_cells(h, icase, h->split_delta, delta);
 }
+
 int gd2d_cells_to_nodes(gd2d_handle *h) {
     if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");
-    return fail(h, GD2D_ERR_STATE, "gd2d_cells_to_nodes: not built yet");
+    int rc = split_buffers(h);
+    if (rc) return rc;
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, false, 0, h->m.Nn, h->lc, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return GD2D_OK;
 }
-int gd2d_calc_diff_term(gd2d_handle *h, int32_t icase, double *) {
+
+int gd2d_calc_diff_term(gd2d_handle *h, int32_t icase, double *diff) {
     int rc = ensure_case(h, icase);
     if (rc) return rc;
-    return fail(h, GD2D_ERR_STATE, "gd2d_calc_diff_term: not built yet");
+    if ((rc = split_buffers(h))) return rc;
+    if (!h->visc) return fail(h, GD2D_ERR_STATE, "the handle was set up without a viscosity model");
+    cudaSetDevice(h->device);
+    CUDA_TRY(h, launch_visc_grad_f64(h->m, h->s, h->lc, h->stream));
+    CUDA_TRY(h, launch_diff_only_f64(h->m, h->s, h->split_diff, h->lc, h->stream));
+    h->split_diff_valid = true;
+    return download_cells(h, icase, h->split_diff, diff);
 }
 int gd2d_autotune(gd2d_handle *h, int32_t, gd2d_launch *) {
     if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");

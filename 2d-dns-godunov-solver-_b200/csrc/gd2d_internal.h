@@ -95,6 +95,13 @@ struct DevMesh {
     const int32_t *tile_case;            // [ntiles]
     const int32_t *node_case;            // [Nn] (viscous only)
     const DevCase *cases;
+    // mixed precision: FP32 copies of the geometry (the FP64 planes are not allocated)
+    const float *nxf, *nyf, *lenf;       // [nfmax][Nc]
+    const float *rareaf, *areaf, *hxf, *charlenf;
+};
+
+struct NodeGradF {  // FP32 node means of the first gradients
+    float2 ru, rv, re;
 };
 
 struct DevState {
@@ -111,6 +118,12 @@ struct DevState {
     unsigned int *node_done;
     int32_t ring_len;
     int32_t pad_;
+    // mixed precision: FP32 primitives for the gathers (U stays FP64)
+    float4 *primf;     // [2][Nc]
+    float4 *nodePf;    // [Nn]
+    float4 *nodeCf;    // [Nn] (viscous)
+    NodeGradF *g1f;    // [Nc] (viscous)
+    NodeGradF *nodeGf; // [Nn] (viscous)
 };
 
 struct LaunchCfg {
@@ -132,5 +145,25 @@ cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, 
 cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,
                                   cudaStream_t st);
+
+// The reference's functions one at a time (FP64, kernels_f64.cu).
+cudaError_t launch_stage_only_f64(const DevMesh &m, const DevState &s, int flux, bool quads, double beta, double dt,
+                                  double t, const double4 *diffs, double4 *unew, double4 *fluxes, const LaunchCfg &lc,
+                                  cudaStream_t st);
+cudaError_t launch_update_only_f64(const DevMesh &m, const DevState &s, double4 *unew, double4 *delta,
+                                   const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_diff_only_f64(const DevMesh &m, const DevState &s, double4 *diffs, const LaunchCfg &lc,
+                                 cudaStream_t st);
+
+// Launchers implemented in kernels_mixed.cu (FP32 reconstruction, fluxes and
+// viscous terms; FP64 state update and reductions).
+cudaError_t launch_cell_step_mixed(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
+                                   const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_node_avg_mixed(const DevMesh &m, const DevState &s, bool visc, bool flip_parity,
+                                  bool zero_prims, int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_visc_grad_mixed(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);
+// U holds the case's FP64 primitives on entry and its conservatives on exit.
+cudaError_t launch_init_state_mixed(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1,
+                                    const LaunchCfg &lc, cudaStream_t st);
 
 }  // namespace gd2d

@@ -74,4 +74,31 @@ cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t
     return cudaGetLastError();
 }
 
+cudaError_t launch_stage_only_f64(const DevMesh &m, const DevState &s, int flux, bool quads, double beta, double dt,
+                                  double t, const double4 *diffs, double4 *unew, double4 *fluxes, const LaunchCfg &lc,
+                                  cudaStream_t st) {
+    const int grid = (int)m.ntiles, b = lc.block;
+#define GD2D_STAGE(F)                                                                                    \
+    (quads ? (k_stage_only<F, true><<<grid, b, 0, st>>>(m, s, beta, dt, t, diffs, unew, fluxes), 0)      \
+           : (k_stage_only<F, false><<<grid, b, 0, st>>>(m, s, beta, dt, t, diffs, unew, fluxes), 0))
+    if (flux == FLUX_ROE) GD2D_STAGE(FLUX_ROE);
+    else if (flux == FLUX_AUSM_M2020) GD2D_STAGE(FLUX_AUSM_M2020);
+    else GD2D_STAGE(FLUX_AUSM);
+#undef GD2D_STAGE
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update_only_f64(const DevMesh &m, const DevState &s, double4 *unew, double4 *delta,
+                                   const LaunchCfg &lc, cudaStream_t st) {
+    k_update_only<<<(int)m.ntiles, lc.block, 0, st>>>(m, s, unew, delta);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diff_only_f64(const DevMesh &m, const DevState &s, double4 *diffs, const LaunchCfg &lc,
+                                 cudaStream_t st) {
+    if (m.nfmax == 4) k_diff_only<true><<<(int)m.ntiles, lc.block, 0, st>>>(m, s, diffs);
+    else k_diff_only<false><<<(int)m.ntiles, lc.block, 0, st>>>(m, s, diffs);
+    return cudaGetLastError();
+}
+
 }  // namespace gd2d

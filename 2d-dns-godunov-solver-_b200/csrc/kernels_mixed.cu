@@ -1,0 +1,403 @@
+// Mixed-precision step kernels: FP32 gathers, reconstruction, face fluxes
+// and viscous terms (FP32 geometry and primitives), FP64 conservative state,
+// Euler-update accumulation, primitive recovery and all reductions.
+//
+// Same dataflow as the FP64 kernels (step_kernels.cuh), with the primitives
+// packed as float4 so each neighbour or node gather is one 128-bit load.
+// Built with fast FP32 division and square root; the error of this path is
+// reported against the FP64 oracle rather than asserted bit-exact.
+#include "step_kernels.cuh"
+
+namespace gd2d {
+
+namespace {
+
+// computeInterfaceSlope (computeslope2d.jl:3-136) in FP32.
+template <int FLUX, bool QUAD>
+__device__ __forceinline__ void face_flux_f(const DevMesh &m, const DevCase &P, const float4 *__restrict__ pin,
+                                            const float4 *__restrict__ nodeP, int64_t g, int k, int nbk, int dnk,
+                                            int upk, int dn2k, int up2k, bool is_quad, const float *uL, float hx_own,
+                                            double t, float g2, float *f) {
+    const int64_t o = (int64_t)k * m.Nc + g;
+    const float side = m.lenf[o], nx = m.nxf[o], ny = m.nyf[o];
+    float uR[4], uUp[4], uDn[4];
+    float hxR = hx_own;
+    if (nbk >= 0) {
+        if (QUAD && is_quad) {
+            float4 a = nodeP[upk], a2 = nodeP[up2k], b = nodeP[dnk], b2 = nodeP[dn2k];
+            uUp[0] = 0.5f * (a.x + a2.x); uUp[1] = 0.5f * (a.y + a2.y);
+            uUp[2] = 0.5f * (a.z + a2.z); uUp[3] = 0.5f * (a.w + a2.w);
+            uDn[0] = 0.5f * (b.x + b2.x); uDn[1] = 0.5f * (b.y + b2.y);
+            uDn[2] = 0.5f * (b.z + b2.z); uDn[3] = 0.5f * (b.w + b2.w);
+        } else {
+            float4 a = nodeP[upk], b = nodeP[dnk];
+            uUp[0] = a.x; uUp[1] = a.y; uUp[2] = a.z; uUp[3] = a.w;
+            uDn[0] = b.x; uDn[1] = b.y; uDn[2] = b.z; uDn[3] = b.w;
+        }
+        float4 r = pin[nbk];
+        uR[0] = r.x; uR[1] = r.y; uR[2] = r.z; uR[3] = r.w;
+        if (P.limiter == LIM_VENKAT) hxR = m.hxf[nbk];
+    } else {
+        bc_ghost<float>(P, m, -nbk - 1, g, k, uL, nx, ny, t, uR);
+        for (int v = 0; v < 4; ++v) { uDn[v] = uL[v]; uUp[v] = uR[v]; }
+    }
+    float UpL[4], UpR[4];
+    if (P.limiter == LIM_VENKAT) {
+        const float K = (float)P.venkat_K;
+        const float KL = K * hx_own, KR = K * hxR;
+        const float e2L = KL * KL * KL, e2R = KR * KR * KR;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const float sc = 0.5f * (uL[v] * uL[v] + uR[v] * uR[v]);
+            UpL[v] = uL[v] + 0.5f * lim_venkat(uL[v] - uDn[v], uR[v] - uL[v], e2L * sc);
+            UpR[v] = uR[v] + 0.5f * lim_venkat(uR[v] - uUp[v], uL[v] - uR[v], e2R * sc);
+        }
+    } else {
+        const int lk = P.limiter;
+        const float ksi = (float)P.ksi;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            UpL[v] = uL[v] + 0.5f * limiter(lk, uL[v] - uDn[v], uR[v] - uL[v], ksi);
+            UpR[v] = uR[v] - 0.5f * limiter(lk, uR[v] - uL[v], uUp[v] - uR[v], ksi);
+        }
+    }
+    face_flux_fn<FLUX, float>(UpR, UpL, nx, ny, side, (float)P.gamma, g2, f);
+}
+
+// Diffusion source (calcDiffTerm.jl:88-113 and the extension models) in FP32.
+template <bool QUAD>
+__device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
+                                              bool is_quad, const float4 &me, float *diff) {
+    const int nf = (QUAD && is_quad) ? 4 : 3;
+    float sx[3] = {0.f, 0.f, 0.f}, sy[3] = {0.f, 0.f, 0.f};
+    float du = 0.f, dv = 0.f;
+    const bool art = (P.visc_model != VISC_REFERENCE) && P.art_visc;
+    for (int k = 0; k < nf; ++k) {
+        const int64_t o = (int64_t)k * m.Nc + g;
+        const float side = m.lenf[o], nx = m.nxf[o], ny = m.nyf[o];
+        const int2 e = m.c2n[o];
+        const NodeGradF A = s.nodeGf[e.x], B = s.nodeGf[e.y];
+        sx[0] += 0.5f * (A.ru.x + B.ru.x) * -ny * side; sy[0] += 0.5f * (A.ru.y + B.ru.y) * -nx * side;
+        sx[1] += 0.5f * (A.rv.x + B.rv.x) * -ny * side; sy[1] += 0.5f * (A.rv.y + B.rv.y) * -nx * side;
+        sx[2] += 0.5f * (A.re.x + B.re.x) * -ny * side; sy[2] += 0.5f * (A.re.y + B.re.y) * -nx * side;
+        if (art) {
+            const float4 na = s.nodePf[e.x], nb = s.nodePf[e.y];
+            du += 0.5f * (na.y + nb.y) * -nx * side;
+            dv += 0.5f * (na.z + nb.z) * -ny * side;
+        }
+    }
+    const float rA = m.rareaf[g];
+    float lap[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) lap[v] = (sx[v] + sy[v]) * rA;
+    const float T = me.w / me.x / (float)P.R;
+    diff[0] = 0.f;
+    if (P.visc_model == VISC_REFERENCE) {
+        const float mu = (float)P.mu_ref;
+        diff[1] = mu * lap[0];
+        diff[2] = mu * lap[1];
+        diff[3] = mu * (float)air_conductivity((double)T) * lap[2];
+    } else {
+        const float mu = (P.visc_model == VISC_SUTHERLAND)
+                             ? (float)P.mu_ref * (sutherland(T) / (float)P.suth_ref)
+                             : (float)P.mu_ref;
+        float mart = 0.f;
+        if (art) {
+            const float HX = m.hxf[g];
+            const float divU = (du + dv) * rA;
+            const float aS = sqrtf((float)P.gamma * me.w / me.x);
+            const float a = 0.05f * aS / HX * 0.70710678f;
+            if (-divU > a) {
+                const float tmp = divU * divU - a * a;
+                if (tmp > 0.f) mart = 0.5f * me.x * (HX * HX * 0.5f) * sqrtf(tmp) * 1.0e-5f;
+            }
+        }
+        const float mue = mu + mart;
+        diff[1] = mue * lap[0];
+        diff[2] = mue * lap[1];
+        diff[3] = mue * lap[2];
+    }
+}
+
+template <int FLUX, bool VISC, bool QUAD, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, const DevState s) {
+    __shared__ Part sh[8];
+    const int par = *s.parity;
+    const float4 *__restrict__ pin = s.primf + (int64_t)par * m.Nc;
+    float4 *__restrict__ pout = s.primf + (int64_t)(par ^ 1) * m.Nc;
+    const float4 *__restrict__ nodeP = s.nodePf;
+    for (int64_t tile = blockIdx.x; tile < m.ntiles; tile += gridDim.x) {
+        const int c = m.tile_case[tile];
+        const DevCase &P = m.cases[c];
+        const double dt = s.cstate[c].dt, t = s.cstate[c].t;
+        const int64_t g = tile * blockDim.x + threadIdx.x;
+        Part part;
+        part.init();
+        const int4 nb = m.nbr[g];
+        if (nb.x != kAbsent) {
+            const bool is_quad = QUAD && (nb.w != kAbsent);
+            const float4 me = pin[g];
+            const float uL[4] = {me.x, me.y, me.z, me.w};
+            const float gam = (float)P.gamma;
+            const float g2 = 2.f * (gam - 1.f) / (gam + 1.f);
+            const float hx_own = (P.limiter == LIM_VENKAT) ? m.hxf[g] : 0.f;
+            const int4 dn = m.dn[g], up = m.up[g];
+            int4 dn2 = make_int4(0, 0, 0, 0), up2 = make_int4(0, 0, 0, 0);
+            if (QUAD && is_quad) { dn2 = m.dn2[g]; up2 = m.up2[g]; }
+            float F[4], f[4];
+            face_flux_f<FLUX, QUAD>(m, P, pin, nodeP, g, 0, nb.x, dn.x, up.x, dn2.x, up2.x, is_quad, uL, hx_own, t, g2, F);
+            face_flux_f<FLUX, QUAD>(m, P, pin, nodeP, g, 1, nb.y, dn.y, up.y, dn2.y, up2.y, is_quad, uL, hx_own, t, g2, f);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) F[v] += f[v];
+            face_flux_f<FLUX, QUAD>(m, P, pin, nodeP, g, 2, nb.z, dn.z, up.z, dn2.z, up2.z, is_quad, uL, hx_own, t, g2, f);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) F[v] += f[v];
+            if (QUAD && is_quad) {
+                face_flux_f<FLUX, QUAD>(m, P, pin, nodeP, g, 3, nb.w, dn.w, up.w, dn2.w, up2.w, is_quad, uL, hx_own, t, g2, f);
+#pragma unroll
+                for (int v = 0; v < 4; ++v) F[v] += f[v];
+            }
+            float diff[4] = {0.f, 0.f, 0.f, 0.f};
+            if (VISC) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
+            // FP32 increment, FP64 accumulation of the Euler update
+            const float bdt = (float)(P.beta * dt);
+            const float rarea = m.rareaf[g];
+            const double4 U = s.U[g];
+            const double Uo[4] = {U.x, U.y, U.z, U.w};
+            double Un[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Un[v] = Uo[v] + (double)(bdt * (diff[v] - F[v] * rarea));
+            if (P.density_constrained == 1) {
+                if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
+                if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
+            }
+            s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
+            // primitives from the FP64 state
+            const double rho = Un[0];
+            const double rinv = 1.0 / rho;
+            const double ux = Un[1] * rinv;
+            const double uy = Un[2] * rinv;
+            const double p = (P.gamma - 1.0) * (Un[3] - 0.5 * (Un[1] * ux + Un[2] * uy));
+            const float a = sqrtf((float)(P.gamma * p * rinv));
+            const float vmax = sqrtf((float)(ux * ux + uy * uy)) + a;
+            pout[g] = make_float4((float)rho, (float)ux, (float)uy, (float)p);
+            const double area = (double)m.areaf[g];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const double d = Un[v] - Uo[v];
+                part.res[v] = d * d;
+                part.tot[v] = Un[v] * area;
+            }
+            part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
+            part.vmax = (double)vmax;
+            part.rmin = (double)(m.charlenf[g] / vmax);
+            part.rhomin = (double)me.x;
+            part.rhomax = (double)me.x;
+            const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
+                            (p > 0.0);
+            part.bad = ok ? 0.0 : 1.0;
+        }
+        tile_epilogue(m, s, tile, c, part, sh, false);
+    }
+}
+
+template <bool VISC, bool UNIT>
+__global__ void __launch_bounds__(256) k_node_avg_mixed(const DevMesh m, const DevState s, int flip, int zero_prims,
+                                                        int64_t n0, int64_t n1) {
+    const int par = *s.parity;
+    const float4 *__restrict__ src = s.primf + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
+    const int W = m.cluster_w;
+    for (int64_t J = n0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < n1; J += (int64_t)gridDim.x * blockDim.x) {
+        bool prim_form = false;
+        float gop = 0.f, gam = 0.f;
+        if (VISC) {
+            const DevCase &P = m.cases[m.node_case[J]];
+            prim_form = P.visc_model != VISC_REFERENCE;
+            gop = (float)P.gamma_over_Pr;
+            gam = (float)P.gamma;
+        }
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, det = 0.f;
+        float c0 = 0.f, c1 = 0.f, c2 = 0.f;
+        int cnt = 0;
+        for (int j = 0; j < W; ++j) {
+            const int c = m.cl[(int64_t)j * m.Nn + J];
+            if (c >= 0) {
+                const float w = UNIT ? 1.f : (float)m.wt[(int64_t)j * m.Nn + J];
+                const float4 p = src[c];
+                a0 += p.x * w; a1 += p.y * w; a2 += p.z * w; a3 += p.w * w;
+                det += w;
+                if (VISC) {
+                    if (prim_form) {
+                        c0 += p.y; c1 += p.z; c2 += 0.5f * (p.y * p.y + p.z * p.z) + gop * (p.w / ((gam - 1.f) * p.x));
+                    } else {
+                        const double4 u = s.U[c];
+                        c0 += (float)u.y; c1 += (float)u.z; c2 += (float)u.w;
+                    }
+                    ++cnt;
+                }
+            }
+        }
+        if (det != 0.f) { const float r = 1.f / det; a0 *= r; a1 *= r; a2 *= r; a3 *= r; }
+        s.nodePf[J] = zero_prims ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(a0, a1, a2, a3);
+        if (VISC) {
+            const float r = cnt ? 1.f / (float)cnt : 0.f;
+            s.nodeCf[J] = make_float4(c0 * r, c1 * r, c2 * r, 0.f);
+        }
+    }
+    if (flip) {
+        __shared__ int s_last;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            unsigned int prev = atomicAdd(s.node_done, 1u);
+            s_last = (prev == gridDim.x - 1u) ? 1 : 0;
+        }
+        __syncthreads();
+        if (s_last && threadIdx.x == 0) {
+            *s.node_done = 0u;
+            *s.parity = par ^ 1;
+        }
+    }
+}
+
+template <bool QUAD>
+__global__ void __launch_bounds__(256) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
+    for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
+        const int4 nb = m.nbr[g];
+        if (nb.x == kAbsent) continue;
+        const int nf = (QUAD && nb.w != kAbsent) ? 4 : 3;
+        float sx[3] = {0.f, 0.f, 0.f}, sy[3] = {0.f, 0.f, 0.f};
+        for (int k = 0; k < nf; ++k) {
+            const int64_t o = (int64_t)k * m.Nc + g;
+            const float side = m.lenf[o], nx = m.nxf[o], ny = m.nyf[o];
+            const int2 e = m.c2n[o];
+            const float4 A = s.nodeCf[e.x], B = s.nodeCf[e.y];
+            sx[0] += 0.5f * (A.x + B.x) * -ny * side; sy[0] += 0.5f * (A.x + B.x) * -nx * side;
+            sx[1] += 0.5f * (A.y + B.y) * -ny * side; sy[1] += 0.5f * (A.y + B.y) * -nx * side;
+            sx[2] += 0.5f * (A.z + B.z) * -ny * side; sy[2] += 0.5f * (A.z + B.z) * -nx * side;
+        }
+        const float rA = m.rareaf[g];
+        NodeGradF r;
+        r.ru = make_float2(sx[0] * rA, sy[0] * rA);
+        r.rv = make_float2(sx[1] * rA, sy[1] * rA);
+        r.re = make_float2(sx[2] * rA, sy[2] * rA);
+        s.g1f[g] = r;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_grad1_nodes_mixed(const DevMesh m, const DevState s) {
+    const int W = m.cluster_w;
+    for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
+        float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int cnt = 0;
+        for (int j = 0; j < W; ++j) {
+            const int c = m.cl[(int64_t)j * m.Nn + J];
+            if (c >= 0) {
+                const NodeGradF q = s.g1f[c];
+                v[0] += q.ru.x; v[1] += q.ru.y; v[2] += q.rv.x; v[3] += q.rv.y; v[4] += q.re.x; v[5] += q.re.y;
+                ++cnt;
+            }
+        }
+        const float r = cnt ? 1.f / (float)cnt : 0.f;
+        NodeGradF o;
+        o.ru = make_float2(v[0] * r, v[1] * r);
+        o.rv = make_float2(v[2] * r, v[3] * r);
+        o.re = make_float2(v[4] * r, v[5] * r);
+        s.nodeGf[J] = o;
+    }
+}
+
+// U holds FP64 primitives on entry: conservatives (utilsFVM2dp.jl:4-17) and
+// the FP32 primitives are written, with the first dt's reductions.
+__global__ void __launch_bounds__(256) k_init_state_mixed(const DevMesh m, const DevState s, int64_t t0, int64_t t1) {
+    __shared__ Part sh[8];
+    const int par = *s.parity;
+    float4 *__restrict__ pout = s.primf + (int64_t)par * m.Nc;
+    for (int64_t tile = t0 + blockIdx.x; tile < t1; tile += gridDim.x) {
+        const int c = m.tile_case[tile];
+        const DevCase &P = m.cases[c];
+        const int64_t g = tile * blockDim.x + threadIdx.x;
+        Part part;
+        part.init();
+        const int4 nb = m.nbr[g];
+        if (nb.x != kAbsent) {
+            const double4 q = s.U[g];
+            const double G = P.gamma;
+            const double r = q.x, u = q.y, v = q.z, pp = q.w;
+            s.U[g] = make_double4(r, r * u, r * v, pp / (G - 1.0) + 0.5 * r * (u * u + v * v));
+            pout[g] = make_float4((float)r, (float)u, (float)v, (float)pp);
+            const double a = sqrt(G * pp / r);
+            const double vmax = sqrt(u * u + v * v) + a;
+            part.vmax = vmax;
+            part.rmin = (double)m.charlenf[g] / vmax;
+        }
+        tile_epilogue(m, s, tile, c, part, sh, true);
+    }
+}
+
+int grid_for_m(int64_t work, int block) {
+    int64_t g = (work + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 148LL * 64) g = 148 * 64;
+    return (int)g;
+}
+
+template <int FLUX, bool VISC, bool QUAD>
+cudaError_t cell_step_m(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
+    int grid = lc.persistent ? lc.grid : (int)m.ntiles;
+    if (lc.min_blocks >= 4) k_cell_step_mixed<FLUX, VISC, QUAD, 4><<<grid, lc.block, 0, st>>>(m, s);
+    else if (lc.min_blocks == 3) k_cell_step_mixed<FLUX, VISC, QUAD, 3><<<grid, lc.block, 0, st>>>(m, s);
+    else k_cell_step_mixed<FLUX, VISC, QUAD, 2><<<grid, lc.block, 0, st>>>(m, s);
+    return cudaGetLastError();
+}
+
+template <int FLUX>
+cudaError_t cell_step_flux_m(const DevMesh &m, const DevState &s, bool visc, bool quads, const LaunchCfg &lc,
+                             cudaStream_t st) {
+    if (visc) return quads ? cell_step_m<FLUX, true, true>(m, s, lc, st) : cell_step_m<FLUX, true, false>(m, s, lc, st);
+    return quads ? cell_step_m<FLUX, false, true>(m, s, lc, st) : cell_step_m<FLUX, false, false>(m, s, lc, st);
+}
+
+}  // namespace
+
+cudaError_t launch_cell_step_mixed(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
+                                   const LaunchCfg &lc, cudaStream_t st) {
+    switch (flux) {
+    case FLUX_ROE: return cell_step_flux_m<FLUX_ROE>(m, s, visc, quads, lc, st);
+    case FLUX_AUSM_M2020: return cell_step_flux_m<FLUX_AUSM_M2020>(m, s, visc, quads, lc, st);
+    default: return cell_step_flux_m<FLUX_AUSM>(m, s, visc, quads, lc, st);
+    }
+}
+
+cudaError_t launch_node_avg_mixed(const DevMesh &m, const DevState &s, bool visc, bool flip_parity, bool zero_prims,
+                                  int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st) {
+    const int b = lc.node_block;
+    const int grid = grid_for_m(n1 - n0, b);
+    const bool unit = m.unit_weights != 0;
+    if (visc) {
+        if (unit) k_node_avg_mixed<true, true><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+        else k_node_avg_mixed<true, false><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+    } else {
+        if (unit) k_node_avg_mixed<false, true><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+        else k_node_avg_mixed<false, false><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_visc_grad_mixed(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
+    const int b = lc.node_block;
+    if (m.nfmax == 4) k_grad1_cells_mixed<true><<<grid_for_m(m.Nc, b), b, 0, st>>>(m, s);
+    else k_grad1_cells_mixed<false><<<grid_for_m(m.Nc, b), b, 0, st>>>(m, s);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_grad1_nodes_mixed<<<grid_for_m(m.Nn, b), b, 0, st>>>(m, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_state_mixed(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,
+                                    cudaStream_t st) {
+    k_init_state_mixed<<<(int)(t1 - t0), lc.block, 0, st>>>(m, s, t0, t1);
+    return cudaGetLastError();
+}
+
+}  // namespace gd2d

@@ -82,7 +82,7 @@ __device__ __forceinline__ void block_reduce(Part &p, Part *sh) {
 // reduce the tile records in a fixed order, publish the step statistics and
 // advance time (flowTime += dt, testInviscidFluxesGPUx32.jl:401) and the
 // next dt (tau at :322-324, or the local-CFL extension).
-__device__ void finalize_case(const DevMesh &m, const DevState &s, int c, Part *sh, bool is_init) {
+static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c, Part *sh, bool is_init) {
     const DevCase &P = m.cases[c];
     Part acc;
     acc.init();
@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(256) k_grad1_cells(const DevMesh m, const DevS
 
 // Unweighted node means of the first gradients (calcPhiInCellCluster on the
 // gradient fields, calcGradients.jl:3-18).
-__global__ void __launch_bounds__(256) k_grad1_nodes(const DevMesh m, const DevState s) {
+static __global__ void __launch_bounds__(256) k_grad1_nodes(const DevMesh m, const DevState s) {
     const int W = m.cluster_w;
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(256) k_grad1_nodes(const DevMesh m, const DevS
 
 // phs2dcns2dcellsSA (utilsFVM2dp.jl:4-17) on the current primitives and the
 // reductions that give the first step's dt (createFields2d's VMAX).
-__global__ void __launch_bounds__(256) k_init_state(const DevMesh m, const DevState s, int64_t t0, int64_t t1) {
+static __global__ void __launch_bounds__(256) k_init_state(const DevMesh m, const DevState s, int64_t t0, int64_t t1) {
     __shared__ Part sh[8];
     const int par = *s.parity;
     const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
@@ -504,6 +504,98 @@ __global__ void __launch_bounds__(256) k_init_state(const DevMesh m, const DevSt
         }
         tile_epilogue(m, s, tile, c, part, sh, true);
     }
+}
+
+// ------------------------------------ the reference's functions one at a time
+
+// calcOneStageMUSCLcpuFast alone (calcOneStageMUSCLcpuFast.jl:3-107): FLUXES
+// and Unew from the current primitives, node primitives, Uold and Diff
+// (diff may be NULL: zero), with the caller's beta, dt and flowTime.  One
+// tile of blockDim cells per block, as the fused kernel.
+template <int FLUX, bool QUAD>
+__global__ void __launch_bounds__(256) k_stage_only(const DevMesh m, const DevState s, double beta, double dt,
+                                                    double t, const double4 *__restrict__ diffs,
+                                                    double4 *__restrict__ unew, double4 *__restrict__ fluxes) {
+    const int par = *s.parity;
+    const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
+    const int64_t tile = blockIdx.x;
+    const int c = m.tile_case[tile];
+    const DevCase &P = m.cases[c];
+    const int64_t g = tile * blockDim.x + threadIdx.x;
+    const int4 nb = m.nbr[g];
+    if (nb.x == kAbsent) return;
+    const bool is_quad = QUAD && (nb.w != kAbsent);
+    const double4 me = pin[g];
+    const double uL[4] = {me.x, me.y, me.z, me.w};
+    const double gam = P.gamma;
+    const double g2 = 2.0 * (gam - 1.0) / (gam + 1.0);
+    const double hx_own = (P.limiter == LIM_VENKAT) ? m.hx[g] : 0.0;
+    const int4 dn = m.dn[g], up = m.up[g];
+    int4 dn2 = make_int4(0, 0, 0, 0), up2 = make_int4(0, 0, 0, 0);
+    if (QUAD && is_quad) { dn2 = m.dn2[g]; up2 = m.up2[g]; }
+    double F[4], f[4];
+    face_flux<FLUX, QUAD>(m, P, pin, s.nodeP, g, 0, nb.x, dn.x, up.x, dn2.x, up2.x, is_quad, uL, hx_own, t, g2, F);
+    face_flux<FLUX, QUAD>(m, P, pin, s.nodeP, g, 1, nb.y, dn.y, up.y, dn2.y, up2.y, is_quad, uL, hx_own, t, g2, f);
+    for (int v = 0; v < 4; ++v) F[v] = F[v] + f[v];
+    face_flux<FLUX, QUAD>(m, P, pin, s.nodeP, g, 2, nb.z, dn.z, up.z, dn2.z, up2.z, is_quad, uL, hx_own, t, g2, f);
+    for (int v = 0; v < 4; ++v) F[v] = F[v] + f[v];
+    if (QUAD && is_quad) {
+        face_flux<FLUX, QUAD>(m, P, pin, s.nodeP, g, 3, nb.w, dn.w, up.w, dn2.w, up2.w, is_quad, uL, hx_own, t, g2, f);
+        for (int v = 0; v < 4; ++v) F[v] = F[v] + f[v];
+    }
+    double diff[4] = {0.0, 0.0, 0.0, 0.0};
+    if (diffs) {
+        const double4 d = diffs[g];
+        diff[0] = d.x; diff[1] = d.y; diff[2] = d.z; diff[3] = d.w;
+    }
+    const double rarea = m.rarea[g];
+    const double4 U = s.U[g];
+    const double Uo[4] = {U.x, U.y, U.z, U.w};
+    double Un[4];
+    for (int v = 0; v < 4; ++v) Un[v] = (Uo[v] - F[v] * beta * dt * rarea + beta * dt * diff[v]);
+    unew[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
+    fluxes[g] = make_double4(F[0], F[1], F[2], F[3]);
+}
+
+// updateVariablesSA alone (evaluate2d.jl:52-110): primitives of Unew in
+// place, Delta = Unew - Uold, Uold <- Unew (density clamp as configured).
+static __global__ void __launch_bounds__(256) k_update_only(const DevMesh m, const DevState s, double4 *__restrict__ unew,
+                                                     double4 *__restrict__ delta) {
+    const int par = *s.parity;
+    double4 *__restrict__ prim = s.prim + (int64_t)par * m.Nc;
+    const int64_t tile = blockIdx.x;
+    const DevCase &P = m.cases[m.tile_case[tile]];
+    const int64_t g = tile * blockDim.x + threadIdx.x;
+    if (m.nbr[g].x == kAbsent) return;
+    double4 un = unew[g];
+    if (P.density_constrained == 1) {
+        if (un.x >= P.rho_max) un.x = P.rho_max;
+        if (un.x <= P.rho_min) un.x = P.rho_min;
+        unew[g] = un;
+    }
+    const double G = P.gamma;
+    const double rho = un.x, ux = un.y / un.x, uy = un.z / un.x;
+    const double p = (G - 1.0) * (un.w - 0.5 * (un.y * un.y + un.z * un.z) / un.x);
+    prim[g] = make_double4(rho, ux, uy, p);
+    const double4 uo = s.U[g];
+    delta[g] = make_double4(un.x - uo.x, un.y - uo.y, un.z - uo.z, un.w - uo.w);
+    s.U[g] = un;
+}
+
+// calcDiffTerm alone (calcDiffTerm.jl:31-121): the diffusion source from
+// the first-gradient node means (the grad1 passes must have run).
+template <bool QUAD>
+__global__ void __launch_bounds__(256) k_diff_only(const DevMesh m, const DevState s, double4 *__restrict__ diffs) {
+    const int par = *s.parity;
+    const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
+    const int64_t tile = blockIdx.x;
+    const DevCase &P = m.cases[m.tile_case[tile]];
+    const int64_t g = tile * blockDim.x + threadIdx.x;
+    const int4 nb = m.nbr[g];
+    if (nb.x == kAbsent) return;
+    double diff[4];
+    diff_source<QUAD>(m, s, P, g, QUAD && nb.w != kAbsent, pin[g], diff);
+    diffs[g] = make_double4(diff[0], diff[1], diff[2], diff[3]);
 }
 
 }  // namespace gd2d

@@ -24,7 +24,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC, 
 # (source, extra flags)
 UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
-    ("kernels_mixed.cu", []),
+    ("kernels_mixed.cu", ["-use_fast_math"]),
     ("gd2d_api.cu", []),
     ("gd2d_noalloc.cu", ["-fmad=false"]),
 ]
@@ -57,8 +57,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if f.read().strip() == dig:
                 return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)
-    objs = []
-    for src, extra in UNITS:
+    objs, procs = [], []
+    for src, extra in UNITS:  # translation units compile in parallel
         path = os.path.join(CSRC, src)
         if not os.path.exists(path):
             continue
@@ -66,8 +66,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
         cmd = [NVCC] + ARCH + COMMON + extra + ["-c", path, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.check_call(cmd)
+        procs.append((cmd, subprocess.Popen(cmd)))
         objs.append(obj)
+    for cmd, p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, cmd)
     cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)

@@ -182,6 +182,43 @@ def cpu_reference(pkg, items, steps, warmup, budget_s=25.0):
             "seconds": dt}
 
 
+def mixed_variant(pkg, items, s64, args, peak):
+    """The same workload on the mixed-precision path: device-timed
+    throughput, and the error after --error-steps steps against the FP64 path
+    (bit-identical to the CPU oracle in the parity tests) from the same
+    initial state."""
+    mesh, cfg, prims = items[0]
+    sm = pkg.solver.Solver([mesh], [cfg], pkg.solver.make_launch(precision="mixed", order=args.order))
+    sm.createFields2d(0, *prims)
+    sm.propagate2d(args.warmup)
+    sm.propagate2d(args.steps)
+    tot, cell_ms, _ = sm.last_timing()
+    value = mesh.nCells * args.steps / (tot / 1e3) / 1e6
+    alg = ALG_BYTES[("mixed", True)]
+    # error run: both paths from the initial state
+    n_err = args.error_steps
+    sm.createFields2d(0, *prims)
+    s64.createFields2d(0, *prims)
+    hm = sm.propagate2d(n_err)[0]
+    h64 = s64.propagate2d(n_err)[0]
+    Um = sm.get_state(0)["Ucons"]
+    U64 = s64.get_state(0)["Ucons"]
+    l2 = np.sqrt(((Um - U64) ** 2).sum(axis=0)) / np.sqrt((U64 ** 2).sum(axis=0))
+    linf = np.abs(Um - U64).max(axis=0) / np.abs(U64).max(axis=0)
+    hist_m = sm.history(0)
+    hist_64 = s64.history(0)
+    t0m, t064 = hist_m[0]["totals"], hist_64[0]["totals"]
+    drift = [abs((hm["totals"][v] - t0m[v]) - (h64["totals"][v] - t064[v])) / max(abs(t064[v]), 1e-300)
+             for v in range(4)]
+    sm.close()
+    return {"value": value, "unit": "Mcell-steps/s", "ms_per_step": tot / args.steps, "cell_kernel_ms": cell_ms,
+            "roofline": {"achieved": alg * mesh.nCells / (cell_ms / 1e3) / 1e9 if cell_ms else None, "peak": peak,
+                         "frac": (alg * mesh.nCells / (cell_ms / 1e3) / 1e9 / peak) if cell_ms else None,
+                         "alg_bytes_per_cell": alg},
+            "error_vs_fp64": {"steps": n_err, "l2_rel": [float(x) for x in l2], "linf_rel": [float(x) for x in linf],
+                              "vars": ["rho", "rho_u", "rho_v", "E"], "totals_drift_rel": drift}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -193,6 +230,9 @@ def main():
     ap.add_argument("--order", default="hilbert")
     ap.add_argument("--graph-steps", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    ap.add_argument("--error-steps", type=int, default=1000,
+                    help="steps of the mixed-vs-FP64 error measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -273,6 +313,8 @@ def main():
                          "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak},
             "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "clocks": clocks}
+    if args.config == "cylinder" and args.precision == "f64" and not args.no_mixed:
+        line["mixed"] = mixed_variant(pkg, items, s, args, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(pkg, items, args.steps, args.warmup)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -1,0 +1,70 @@
+"""Mixed-precision path (FP32 reconstruction, fluxes and viscous terms; FP64
+state update and reductions): error against the FP64 CPU oracle.
+
+Reported as the relative L2 and Linf error of rho, rho u, rho v, E after N
+steps and the drift of the conserved totals; the bounds below are the
+acceptance thresholds of this path (north star: density L2 error under 1e-5
+after 1000 steps on the cylinder; here shorter runs on smaller meshes).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def l2_linf(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    l2 = np.sqrt(((a - b) ** 2).sum(axis=0)) / np.maximum(np.sqrt((b ** 2).sum(axis=0)), 1e-300)
+    linf = np.abs(a - b).max(axis=0) / np.maximum(np.abs(b).max(axis=0), 1e-300)
+    return l2, linf
+
+
+def run(pkg, orc, mesh, cfg, prims, nsteps, **launch):
+    s = pkg.setupSolver(mesh, cfg, precision="mixed", **launch)
+    s.createFields2d(0, *prims)
+    gh = s.propagate2d(nsteps)
+    o = orc.Oracle(mesh, cfg, nthreads=4)
+    o.init_fields(*prims)
+    oh = o.run(nsteps)
+    return s, o, s.history(0), oh
+
+
+def test_mixed_square_100_steps(pkg, orc):
+    mesh, cfg, prims = pkg.cases.square_inviscid(101)
+    s, o, gh, oh = run(pkg, orc, mesh, cfg, prims, 100)
+    U = s.get_state(0)["Ucons"]
+    l2, linf = l2_linf(U, o.field("Uold"))
+    print("mixed square 100 steps L2", l2, "Linf", linf)
+    assert l2[0] < 1e-5 and l2.max() < 1e-4
+    # conserved totals follow the FP64 oracle
+    for v in range(4):
+        assert gh[-1]["totals"][v] == pytest.approx(oh[-1]["totals"][v], rel=1e-5, abs=1e-9)
+    assert gh[-1]["dt"] == pytest.approx(oh[-1]["dt"], rel=1e-4)
+
+
+def test_mixed_cylinder_viscous(pkg, orc):
+    mesh, cfg, prims = pkg.cases.cylinder_case(129)
+    s, o, gh, oh = run(pkg, orc, mesh, cfg, prims, 100)
+    U = s.get_state(0)["Ucons"]
+    l2, linf = l2_linf(U, o.field("Uold"))
+    print("mixed cylinder 129 100 steps L2", l2, "Linf", linf)
+    assert l2[0] < 1e-4
+    assert all(h["nonfinite"] == 0 for h in gh)
+
+
+@pytest.mark.parametrize("flux", ["roe", "ausm"])
+def test_mixed_fluxes_tgv_batch(pkg, orc, flux):
+    tg = [pkg.cases.tgv_case(n, 0.2 + 0.1 * k, 400.0 + 300 * k, flux=flux) for k, n in enumerate((33, 49, 41))]
+    s = pkg.solver.Solver([m for m, _, _ in tg], [c for _, c, _ in tg], pkg.solver.make_launch(precision="mixed"))
+    for i, (_, _, p) in enumerate(tg):
+        s.createFields2d(i, *p)
+    s.propagate2d(50)
+    for i, (m, c, p) in enumerate(tg):
+        o = orc.Oracle(m, c, nthreads=2)
+        o.init_fields(*p)
+        oh = o.run(50)
+        l2, _ = l2_linf(s.get_state(i)["Ucons"], o.field("Uold"))
+        assert l2[0] < 1e-5, (flux, i, l2)
+        ek_gpu = s.history(i)[-1]["Ek"]
+        assert ek_gpu == pytest.approx(oh[-1]["Ek"], rel=1e-5)

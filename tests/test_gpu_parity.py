@@ -191,3 +191,43 @@ def test_nonfinite_state_is_reported(pkg):
     with pytest.raises(pkg._native.NativeError) as ei:
         s.propagate2d(3)
     assert ei.value.code == -4
+
+
+def test_single_function_entry_points(pkg, orc):
+    """calcOneStageMUSCLcpuFast, updateVariablesSA,
+    cells2nodesSolutionReconstructionWithStencils and calcDiffTerm called one
+    at a time through the C ABI, against the oracle's functions."""
+    mesh, cfg, prims = pkg.cases.square_inviscid(41)
+    s = pkg.setupSolver(mesh, cfg)
+    s.createFields2d(0, *prims)
+    o = orc.Oracle(mesh, cfg, nthreads=2)
+    o.init_fields(*prims)
+    for it in range(3):
+        dt, t = 2.0e-4, 1.0e-3 * it
+        F, Un = s.calcOneStageMUSCLcpuFast(0, 1.0, dt, t)
+        o.calc_one_stage(1.0, dt, t)
+        assert np.array_equal(F, o.field("FLUXES")) and np.array_equal(Un, o.field("Unew")), it
+        D = s.updateVariablesSA(0)
+        o.update_variables()
+        assert np.array_equal(D, o.field("Delta")), it
+        s.cells2nodesSolutionReconstructionWithStencils()
+        o.cells2nodes()
+        g = s.get_state(0)
+        assert np.array_equal(g["prims"], o.prims()) and np.array_equal(g["node_prims"], o.node_prims()), it
+
+
+@pytest.mark.parametrize("which", ["reference_tgv", "cylinder"])
+def test_calc_diff_term_entry_point(pkg, orc, which):
+    if which == "reference_tgv":
+        mesh, cfg, prims = pkg.cases.reference_tgv_case(33)
+    else:
+        mesh, cfg, prims = pkg.cases.cylinder_case(65)
+    s = pkg.setupSolver(mesh, cfg)
+    s.createFields2d(0, *prims)
+    s.propagate2d(3)  # non-trivial node fields
+    o = orc.Oracle(mesh, cfg, nthreads=2)
+    o.init_fields(*prims)
+    o.run(3)
+    D = s.calcDiffTerm(0)
+    o.calc_diff_term()
+    assert relerr(D, o.field("Diff")) <= TOL_STEP
