@@ -8,6 +8,13 @@ a12 = min of the numerical sound speeds, AUSMflux2dFast.jl:87-175) and Roe
 in 50-digit arithmetic (mpmath), independently of the C oracle, so the
 oracle's double-precision restatement can be checked against it.
 
+It also converts the reference's only shipped mesh, oblickShock2dl00F1n.h5
+(3,838 cells: 3,592 triangles and 246 quads, non-unit node_stencils), with
+the package's HDF5 reader into tests/golden/oblique_shock_mesh.npz so that
+the GPU tests can run the reference's own mesh without the reference
+checkout, and records a digest of every dataset in
+tests/golden/oblique_shock_mesh.json.
+
 Run: python tests/golden/make_golden.py
 """
 import json
@@ -110,6 +117,33 @@ def main():
         json.dump({"source": "testFluxes2d.jl:10-24 pair, 50-digit evaluation (make_golden.py)", "cases": cases}, f,
                   indent=1)
     print("wrote", path)
+    convert_reference_mesh()
+
+
+def convert_reference_mesh(src="/root/reference/oblickShock2dl00F1n.h5"):
+    import hashlib
+    import sys
+    import numpy as np
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(os.path.dirname(here))
+    sys.path.insert(0, root)
+    import __graft_entry__ as graft
+    pkg = graft.load_package()
+    from importlib import import_module
+    h5 = import_module(graft.PKG_NAME + ".hdf5mesh")
+    if not os.path.exists(src):
+        print("reference mesh not found; skipped", src)
+        return
+    ds = h5.read_datasets(src)
+    mesh = h5.readMesh2dHDF5(src)
+    mesh.save_npz(os.path.join(here, "oblique_shock_mesh.npz"))
+    digest = {k: hashlib.sha256(np.ascontiguousarray(np.asarray(v)).tobytes()).hexdigest() for k, v in
+              sorted(ds.items())}
+    meta = {"source": "oblickShock2dl00F1n.h5 (reference repository), read by hdf5mesh.read_datasets",
+            "nCells": int(mesh.nCells), "nNodes": int(mesh.nNodes), "sha256": digest}
+    with open(os.path.join(here, "oblique_shock_mesh.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+    print("wrote oblique_shock_mesh.npz/.json", mesh.nCells, mesh.nNodes)
 
 
 if __name__ == "__main__":
