@@ -81,6 +81,12 @@ struct gd2d_handle {
     int64_t last_launches = 0;
     double4 *pinned = nullptr;  // page-locked staging for state uploads and downloads
     size_t pinned_count = 0;
+    // face-loop variants: faces sorted by colour, colour ranges, flux storage
+    int loop = GD2D_LOOP_CELL;
+    int4 *d_faces = nullptr;
+    int64_t nfaces = 0;
+    std::vector<int64_t> colour_off;
+    double4 *Facc = nullptr, *Fslot = nullptr;
     // single-function entry points
     double4 *split_unew = nullptr, *split_flux = nullptr, *split_delta = nullptr, *split_diff = nullptr;
     bool split_stage_done = false, split_diff_valid = false;
@@ -529,6 +535,53 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     }
     h->tile_case_h = tile_case;
 
+    // face list for the face-loop variants: each interior face once (from its
+    // lower-indexed cell), boundary faces once; greedy edge colouring so that
+    // no two faces of one colour share a cell
+    h->loop = h->launch.loop;
+    std::vector<int4> faces;
+    if (h->loop != GD2D_LOOP_CELL) {
+        const char *bad = (h->loop != GD2D_LOOP_FACE_COLOURED && h->loop != GD2D_LOOP_FACE_SLOTS)
+                              ? "unknown loop variant"
+                              : (h->mixed ? "the face-loop variants run the FP64 path only" : nullptr);
+        if (bad) {
+            if (h->own_stream) cudaStreamDestroy(h->stream);
+            delete h;
+            return fail(nullptr, GD2D_ERR_ARG, "%s", bad);
+        }
+        auto code_k = [](const int4 &v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); };
+        std::vector<uint8_t> used(Nc, 0);
+        std::vector<int> colour;
+        for (int64_t g = 0; g < Nc; ++g) {
+            const int4 nb = nbr[g];
+            if (nb.x == kAbsent) continue;
+            const int nf = nb.w != kAbsent ? 4 : 3;
+            for (int k = 0; k < nf; ++k) {
+                const int code = code_k(nb, k);
+                if (code >= 0 && code < g) continue;
+                int kb = 0;
+                uint8_t mask = used[g];
+                if (code >= 0) {
+                    for (int q = 0; q < 4; ++q)
+                        if (code_k(nbr[code], q) == (int)g) kb = q;
+                    mask |= used[code];
+                }
+                int col = 0;
+                while (mask & (1u << col)) ++col;
+                used[g] |= (uint8_t)(1u << col);
+                if (code >= 0) used[code] |= (uint8_t)(1u << col);
+                faces.push_back(make_int4((int)g, code, k | (kb << 8), col));
+                colour.push_back(col);
+            }
+        }
+        std::stable_sort(faces.begin(), faces.end(), [](const int4 &a, const int4 &b) { return a.w < b.w; });
+        const int ncol = faces.empty() ? 0 : faces.back().w + 1;
+        h->colour_off.assign(ncol + 1, 0);
+        for (const int4 &f : faces) h->colour_off[f.w + 1]++;
+        for (int c = 0; c < ncol; ++c) h->colour_off[c + 1] += h->colour_off[c];
+        h->nfaces = (int64_t)faces.size();
+    }
+
     // ------------------------------------------------------- device
     cudaSetDevice(h->device);
     DevMesh &m = h->m;
@@ -610,6 +663,11 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         if (h->visc) { ALLOC(s.nodeCf, Nn); ALLOC(s.g1f, Nc); ALLOC(s.nodeGf, Nn); }
     }
     ALLOC(s.part, (size_t)ntiles * kPartials);
+    if (h->loop != GD2D_LOOP_CELL) {
+        ALLOC(h->d_faces, faces.size()); UPLOAD(h->d_faces, faces);
+        if (h->loop == GD2D_LOOP_FACE_COLOURED) ALLOC(h->Facc, Nc);
+        else ALLOC(h->Fslot, (size_t)nfmax * Nc);
+    }
     ALLOC(s.cstate, n_cases);
     ALLOC(s.ring, (size_t)s.ring_len * n_cases);
     ALLOC(s.parity, 1);
@@ -729,6 +787,14 @@ int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, do
     return init_case_from_pinned(h, icase, flow_time, rebuild_nodes != 0);
 }
 
+static int64_t kernels_per_step(const gd2d_handle *h) {
+    int64_t n = (h->visc ? 2 : 0) + 1;  // viscous gradient passes, node pass
+    if (h->loop == GD2D_LOOP_FACE_COLOURED) n += (int64_t)h->colour_off.size() - 1 + 1;
+    else if (h->loop == GD2D_LOOP_FACE_SLOTS) n += 2;
+    else n += 1;
+    return n;
+}
+
 // The kernels of one step on the handle's stream: [viscous gradient passes]
 // -> fused cell kernel (bracketed by the optional timing events) -> node pass.
 static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, cudaEvent_t after_cell) {
@@ -739,8 +805,22 @@ static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, 
         if (e != cudaSuccess) return e;
     }
     if (before_cell) cudaEventRecordWithFlags(before_cell, h->stream, cudaEventRecordExternal);
-    e = h->mixed ? launch_cell_step_mixed(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream)
-                 : launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream);
+    if (h->loop == GD2D_LOOP_FACE_COLOURED) {
+        for (size_t c = 0; c + 1 < h->colour_off.size(); ++c) {
+            e = launch_face_flux_f64(h->m, h->s, h->flux, h->quads, false, h->d_faces, h->colour_off[c],
+                                     h->colour_off[c + 1], h->Facc, nullptr, h->lc, h->stream);
+            if (e != cudaSuccess) return e;
+        }
+        e = launch_face_update_f64(h->m, h->s, h->visc, h->quads, false, h->Facc, nullptr, h->lc, h->stream);
+    } else if (h->loop == GD2D_LOOP_FACE_SLOTS) {
+        e = launch_face_flux_f64(h->m, h->s, h->flux, h->quads, true, h->d_faces, 0, h->nfaces, nullptr, h->Fslot,
+                                 h->lc, h->stream);
+        if (e != cudaSuccess) return e;
+        e = launch_face_update_f64(h->m, h->s, h->visc, h->quads, true, nullptr, h->Fslot, h->lc, h->stream);
+    } else {
+        e = h->mixed ? launch_cell_step_mixed(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream)
+                     : launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream);
+    }
     if (e != cudaSuccess) return e;
     if (after_cell) cudaEventRecordWithFlags(after_cell, h->stream, cudaEventRecordExternal);
     return h->mixed ? launch_node_avg_mixed(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream)
@@ -794,12 +874,12 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
                 CUDA_TRY(h, cudaGraphLaunch(h->graph, h->stream));
                 used_graph = true;
                 k += G;
-                launches += (int64_t)G * (h->visc ? 4 : 2);
+                launches += (int64_t)G * kernels_per_step(h);
             }
         }
         for (; k < chunk; ++k) {
             CUDA_TRY(h, launch_step_kernels(h, nullptr, nullptr));
-            launches += h->visc ? 4 : 2;
+            launches += kernels_per_step(h);
         }
         CUDA_TRY(h, cudaEventRecord(h->ev_total[1], h->stream));
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));

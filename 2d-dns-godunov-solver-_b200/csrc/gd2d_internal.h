@@ -146,6 +146,14 @@ cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const Laun
 cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,
                                   cudaStream_t st);
 
+// Face-loop variants (FP64, kernels_f64.cu): fluxes of faces [f0, f1), then
+// the per-cell update.
+cudaError_t launch_face_flux_f64(const DevMesh &m, const DevState &s, int flux, bool quads, bool slots,
+                                 const int4 *faces, int64_t f0, int64_t f1, double4 *Facc, double4 *Fslot,
+                                 const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_face_update_f64(const DevMesh &m, const DevState &s, bool visc, bool quads, bool slots,
+                                   double4 *Facc, const double4 *Fslot, const LaunchCfg &lc, cudaStream_t st);
+
 // The reference's functions one at a time (FP64, kernels_f64.cu).
 cudaError_t launch_stage_only_f64(const DevMesh &m, const DevState &s, int flux, bool quads, double beta, double dt,
                                   double t, const double4 *diffs, double4 *unew, double4 *fluxes, const LaunchCfg &lc,

@@ -74,6 +74,45 @@ cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t
     return cudaGetLastError();
 }
 
+cudaError_t launch_face_flux_f64(const DevMesh &m, const DevState &s, int flux, bool quads, bool slots,
+                                 const int4 *faces, int64_t f0, int64_t f1, double4 *Facc, double4 *Fslot,
+                                 const LaunchCfg &lc, cudaStream_t st) {
+    if (f1 <= f0) return cudaSuccess;
+    const int b = 256;
+    const int grid = (int)((f1 - f0 + b - 1) / b);
+    const int tc = lc.block;
+#define GD2D_FACE(F)                                                                                          \
+    do {                                                                                                      \
+        if (quads) {                                                                                          \
+            if (slots) k_face_flux<F, true, true><<<grid, b, 0, st>>>(m, s, faces, f0, f1, tc, Facc, Fslot);   \
+            else k_face_flux<F, true, false><<<grid, b, 0, st>>>(m, s, faces, f0, f1, tc, Facc, Fslot);        \
+        } else {                                                                                              \
+            if (slots) k_face_flux<F, false, true><<<grid, b, 0, st>>>(m, s, faces, f0, f1, tc, Facc, Fslot);  \
+            else k_face_flux<F, false, false><<<grid, b, 0, st>>>(m, s, faces, f0, f1, tc, Facc, Fslot);       \
+        }                                                                                                     \
+    } while (0)
+    if (flux == FLUX_ROE) GD2D_FACE(FLUX_ROE);
+    else if (flux == FLUX_AUSM_M2020) GD2D_FACE(FLUX_AUSM_M2020);
+    else GD2D_FACE(FLUX_AUSM);
+#undef GD2D_FACE
+    return cudaGetLastError();
+}
+
+cudaError_t launch_face_update_f64(const DevMesh &m, const DevState &s, bool visc, bool quads, bool slots,
+                                   double4 *Facc, const double4 *Fslot, const LaunchCfg &lc, cudaStream_t st) {
+    const int grid = lc.persistent ? lc.grid : (int)m.ntiles;
+#define GD2D_UPD(V, Q, S) k_face_update<V, Q, S, 3><<<grid, lc.block, 0, st>>>(m, s, Facc, Fslot)
+    if (visc) {
+        if (quads) { if (slots) GD2D_UPD(true, true, true); else GD2D_UPD(true, true, false); }
+        else { if (slots) GD2D_UPD(true, false, true); else GD2D_UPD(true, false, false); }
+    } else {
+        if (quads) { if (slots) GD2D_UPD(false, true, true); else GD2D_UPD(false, true, false); }
+        else { if (slots) GD2D_UPD(false, false, true); else GD2D_UPD(false, false, false); }
+    }
+#undef GD2D_UPD
+    return cudaGetLastError();
+}
+
 cudaError_t launch_stage_only_f64(const DevMesh &m, const DevState &s, int flux, bool quads, double beta, double dt,
                                   double t, const double4 *diffs, double4 *unew, double4 *fluxes, const LaunchCfg &lc,
                                   cudaStream_t st) {

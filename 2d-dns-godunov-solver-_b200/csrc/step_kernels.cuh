@@ -506,6 +506,128 @@ static __global__ void __launch_bounds__(256) k_init_state(const DevMesh m, cons
     }
 }
 
+// ------------------------------------------------------- face-loop variants
+
+// One thread per face: the flux seen from cell a (face slot ka), added to a
+// and subtracted from the neighbour b (FACE_COLOURED: into Facc, faces of
+// one launch never share a cell) or stored in the slots (a, ka) and (b, kb)
+// (FACE_SLOTS).  face = (a, neighbour code of slot ka, ka | kb << 8, -).
+template <int FLUX, bool QUAD, bool SLOTS>
+__global__ void __launch_bounds__(256) k_face_flux(const DevMesh m, const DevState s, const int4 *__restrict__ faces,
+                                                   int64_t f0, int64_t f1, int tile_cells,
+                                                   double4 *__restrict__ Facc, double4 *__restrict__ Fslot) {
+    const int64_t f = f0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= f1) return;
+    const int par = *s.parity;
+    const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
+    const int4 fc = faces[f];
+    const int64_t a = fc.x;
+    const int nbk = fc.y, ka = fc.z & 255, kb = fc.z >> 8;
+    const int c = m.tile_case[a / tile_cells];
+    const DevCase &P = m.cases[c];
+    const double t = s.cstate[c].t;
+    const int4 nb = m.nbr[a];
+    const bool is_quad = QUAD && (nb.w != kAbsent);
+    const double4 me = pin[a];
+    const double uL[4] = {me.x, me.y, me.z, me.w};
+    const double gam = P.gamma;
+    const double g2 = 2.0 * (gam - 1.0) / (gam + 1.0);
+    const double hx_own = (P.limiter == LIM_VENKAT) ? m.hx[a] : 0.0;
+    const int4 dn = m.dn[a], up = m.up[a];
+    int4 dn2 = make_int4(0, 0, 0, 0), up2 = make_int4(0, 0, 0, 0);
+    if (QUAD && is_quad) { dn2 = m.dn2[a]; up2 = m.up2[a]; }
+    double fv[4];
+    face_flux<FLUX, QUAD>(m, P, pin, s.nodeP, a, ka, nbk, nbr_k(dn, ka), nbr_k(up, ka), nbr_k(dn2, ka),
+                          nbr_k(up2, ka), is_quad, uL, hx_own, t, g2, fv);
+    if (SLOTS) {
+        Fslot[(int64_t)ka * m.Nc + a] = make_double4(fv[0], fv[1], fv[2], fv[3]);
+        if (nbk >= 0) Fslot[(int64_t)kb * m.Nc + nbk] = make_double4(-fv[0], -fv[1], -fv[2], -fv[3]);
+    } else {
+        double4 x = Facc[a];
+        Facc[a] = make_double4(x.x + fv[0], x.y + fv[1], x.z + fv[2], x.w + fv[3]);
+        if (nbk >= 0) {
+            double4 y = Facc[nbk];
+            Facc[nbk] = make_double4(y.x - fv[0], y.y - fv[1], y.z - fv[2], y.w - fv[3]);
+        }
+    }
+}
+
+// Euler update and updateVariablesSA after a face loop: the cell kernel's
+// second half, with the face-flux sum read back (FACE_SLOTS: summed in face
+// order k = 1..nf as calcOneStageMUSCLcpuFast.jl:66-85; FACE_COLOURED: the
+// accumulator, reset to zero for the next step).
+template <bool VISC, bool QUAD, bool SLOTS, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_face_update(const DevMesh m, const DevState s,
+                                                          double4 *__restrict__ Facc,
+                                                          const double4 *__restrict__ Fslot) {
+    __shared__ Part sh[8];
+    const int par = *s.parity;
+    const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
+    double4 *__restrict__ pout = s.prim + (int64_t)(par ^ 1) * m.Nc;
+    for (int64_t tile = blockIdx.x; tile < m.ntiles; tile += gridDim.x) {
+        const int c = m.tile_case[tile];
+        const DevCase &P = m.cases[c];
+        const double dt = s.cstate[c].dt;
+        const int64_t g = tile * blockDim.x + threadIdx.x;
+        Part part;
+        part.init();
+        const int4 nb = m.nbr[g];
+        if (nb.x != kAbsent) {
+            const bool is_quad = QUAD && (nb.w != kAbsent);
+            const double4 me = pin[g];
+            double F[4];
+            if (SLOTS) {
+                double4 a0 = Fslot[g], a1 = Fslot[m.Nc + g], a2 = Fslot[2 * m.Nc + g];
+                F[0] = a0.x + a1.x + a2.x; F[1] = a0.y + a1.y + a2.y;
+                F[2] = a0.z + a1.z + a2.z; F[3] = a0.w + a1.w + a2.w;
+                if (QUAD && is_quad) {
+                    double4 a3 = Fslot[3 * m.Nc + g];
+                    F[0] = F[0] + a3.x; F[1] = F[1] + a3.y; F[2] = F[2] + a3.z; F[3] = F[3] + a3.w;
+                }
+            } else {
+                double4 a0 = Facc[g];
+                F[0] = a0.x; F[1] = a0.y; F[2] = a0.z; F[3] = a0.w;
+                Facc[g] = make_double4(0.0, 0.0, 0.0, 0.0);
+            }
+            double diff[4] = {0.0, 0.0, 0.0, 0.0};
+            if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
+            const double rarea = m.rarea[g];
+            const double4 U = s.U[g];
+            const double Uo[4] = {U.x, U.y, U.z, U.w};
+            double Un[4];
+            for (int v = 0; v < 4; ++v) Un[v] = (Uo[v] - F[v] * P.beta * dt * rarea + P.beta * dt * diff[v]);
+            if (P.density_constrained == 1) {
+                if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
+                if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
+            }
+            s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
+            const double gam = P.gamma;
+            const double rho = Un[0];
+            const double ux = Un[1] / Un[0];
+            const double uy = Un[2] / Un[0];
+            const double p = (gam - 1.0) * (Un[3] - 0.5 * (Un[1] * Un[1] + Un[2] * Un[2]) / Un[0]);
+            const double a = sqrt(gam * p / rho);
+            const double vmax = sqrt(ux * ux + uy * uy) + a;
+            pout[g] = make_double4(rho, ux, uy, p);
+            const double area = m.area[g];
+            for (int v = 0; v < 4; ++v) {
+                const double d = Un[v] - Uo[v];
+                part.res[v] = d * d;
+                part.tot[v] = Un[v] * area;
+            }
+            part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
+            part.vmax = vmax;
+            part.rmin = m.charlen[g] / vmax;
+            part.rhomin = me.x;
+            part.rhomax = me.x;
+            const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
+                            (p > 0.0);
+            part.bad = ok ? 0.0 : 1.0;
+        }
+        tile_epilogue(m, s, tile, c, part, sh, false);
+    }
+}
+
 // ------------------------------------ the reference's functions one at a time
 
 // calcOneStageMUSCLcpuFast alone (calcOneStageMUSCLcpuFast.jl:3-107): FLUXES

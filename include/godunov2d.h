@@ -59,7 +59,12 @@ enum gd2d_viscosity { GD2D_VISC_NONE = 0, GD2D_VISC_REFERENCE = 1, GD2D_VISC_SUT
 enum gd2d_dt_mode { GD2D_DT_FIXED = 0, GD2D_DT_REFERENCE_TAU = 1, GD2D_DT_LOCAL_CFL = 2 };
 enum gd2d_precision { GD2D_PREC_F64 = 0, GD2D_PREC_MIXED = 1 };
 enum gd2d_order { GD2D_ORDER_NATURAL = 0, GD2D_ORDER_HILBERT = 1, GD2D_ORDER_RCM = 2 };
-enum gd2d_loop { GD2D_LOOP_CELL = 0, GD2D_LOOP_FACE_COLOURED = 1 };
+/* CELL: one thread per cell evaluates its own faces (each interior face
+ * twice, no atomics).  FACE_COLOURED: one thread per face, faces grouped in
+ * colours no two of which touch the same cell, accumulating into the cells.
+ * FACE_SLOTS: one thread per face, each side's flux stored in its own
+ * (cell, face) slot and summed in face order by the update (FP64 only). */
+enum gd2d_loop { GD2D_LOOP_CELL = 0, GD2D_LOOP_FACE_COLOURED = 1, GD2D_LOOP_FACE_SLOTS = 2 };
 
 /* mesh2d_Int32 (primeObjects.jl:109-135) as read by readMesh2dHDF5
  * (utilsIO.jl:107-252).  All matrices column-major. */
