@@ -50,11 +50,15 @@ __device__ __forceinline__ T lim_vanalbada(T a, T b, T c) {
     return (a * (b * b + c) + b * (a * a + c)) / (a * a + b * b + T(2) * c);
 }
 // Venkatakrishnan (JCP 1995) in the two-argument slot (extension):
-// o = outer difference, c = central difference, eps2 = (K*HX)^3.
+// o = outer difference (Delta-), c = central difference (the bound Delta+),
+// eps2 = (K*HX)^3 scaled by the caller; at a local extremum (opposite signs)
+// the bound is zero, which keeps the function continuous in c.
 template <class T>
 __device__ __forceinline__ T lim_venkat(T o, T c, T eps2) {
-    if (o * c <= T(0)) return T(0);
-    return ((c * c + eps2) * o + T(2) * o * o * c) / (c * c + T(2) * o * o + o * c + eps2);
+    if (o * c < T(0)) c = T(0);
+    const T den = c * c + T(2) * o * o + o * c + eps2;
+    if (den == T(0)) return T(0);
+    return ((c * c + eps2) * o + T(2) * o * o * c) / den;
 }
 
 template <class T>

@@ -155,11 +155,16 @@ double orc_vanalbada(double a, double b, double c) {
 
 /* Venkatakrishnan (JCP 1995) smooth limiter in the two-argument slot
  * (extension; the reference has no Venkatakrishnan limiter).  o = outer
- * (upwind) difference, c = central difference, eps2 = (K*HX)^3:
- *   phi = ((c^2+eps2) o + 2 o^2 c) / (c^2 + 2 o^2 + o c + eps2), 0 if o*c <= 0 */
+ * (upwind) difference playing Delta-, c = central difference playing the
+ * bound Delta+, eps2 = (K*HX)^3 (scaled by the caller):
+ *   phi = ((c^2+eps2) o + 2 o^2 c) / (c^2 + 2 o^2 + o c + eps2).
+ * When c has the opposite sign the cell is a local extremum and the bound is
+ * zero (c := 0), which keeps the function continuous in c. */
 double orc_venkat(double o, double c, double eps2) {
-    if (o * c <= 0.0) return 0.0;
-    return ((c * c + eps2) * o + 2.0 * o * o * c) / (c * c + 2.0 * o * o + o * c + eps2);
+    if (o * c < 0.0) c = 0.0;
+    double den = c * c + 2.0 * o * o + o * c + eps2;
+    if (den == 0.0) return 0.0;
+    return ((c * c + eps2) * o + 2.0 * o * o * c) / den;
 }
 
 /* ---------------------------------------------------------------- fluxes */

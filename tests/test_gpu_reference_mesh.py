@@ -20,8 +20,10 @@ def shock_case(pkg, flux="ausm", limiter="minmod"):
     g = 1.4
     cfg = {"thermo": dict(pkg.cases.AIR), "flux": flux, "limiter": limiter, "viscosity": "none", "dt_mode": 2,
            "CFL": 0.4, "beta": 1.0, "ksi": 1.0e-12, "init_nodes": 0,
-           "bc": [{"tag": -1, "kind": "inflow", "rho": 1.0, "u": 2.0, "v": 0.0, "p": 1.0 / g},
-                  {"tag": -2, "kind": "outflow"}, {"tag": -3, "kind": "slip"}, {"tag": -4, "kind": "slip"}]}
+           # tags of the file: -4 left (x=0), -2 right (x=4.1), -3 bottom, -1 top
+           "bc": [{"tag": -4, "kind": "inflow", "rho": 1.0, "u": 2.0, "v": 0.0, "p": 1.0 / g},
+                  {"tag": -1, "kind": "inflow", "rho": 1.0, "u": 2.0, "v": 0.0, "p": 1.0 / g},
+                  {"tag": -2, "kind": "outflow"}, {"tag": -3, "kind": "slip"}]}
     n = mesh.nCells
     xc, yc = mesh.cell_mid_points[:, 0], mesh.cell_mid_points[:, 1]
     rho = 1.0 + 0.1 * np.sin(3 * xc) * np.cos(5 * yc)

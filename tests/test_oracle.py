@@ -90,6 +90,11 @@ def test_venkat_limiter_properties(orc):
     assert L.orc_venkat(1e6, 1.0, 0.0) == pytest.approx(1.0, rel=1e-5)
     assert L.orc_venkat(1.0, 1.0, 0.0) == pytest.approx(0.75)             # phi(1) = 3/4
     assert L.orc_venkat(1e-3, 1e-3, 1.0) == pytest.approx(1e-3, rel=1e-3) # eps dominates: unlimited
+    # continuous across the sign change of the bound (no jump at a local extremum)
+    for eps2 in (0.0, 0.1, 10.0):
+        assert L.orc_venkat(1.0, 1e-13, eps2) == pytest.approx(L.orc_venkat(1.0, -1e-13, eps2), abs=1e-12)
+    # odd in its arguments
+    assert L.orc_venkat(-0.3, -0.7, 0.2) == -L.orc_venkat(0.3, 0.7, 0.2)
 
 
 def test_partition_matches_reference(orc):
