@@ -64,6 +64,51 @@ __device__ __forceinline__ void face_flux_f(const DevMesh &m, const DevCase &P, 
     face_flux_fn<FLUX, float>(UpR, UpL, nx, ny, side, (float)P.gamma, g2, f);
 }
 
+// The same face with every gathered input already in registers: r = the
+// neighbour's primitives, d/u = down/up node primitives (quads: averaged),
+// geometry (nx, ny, side).  Boundary faces ignore r, d, u.
+template <int FLUX>
+__device__ __forceinline__ void face_flux_pre(const DevMesh &m, const DevCase &P, int64_t g, int k, int nbk,
+                                              const float4 &r, const float4 &dd, const float4 &uu, float nx, float ny,
+                                              float side, const float *uL, float hx_own, float hxR, double t, float g2,
+                                              float *f) {
+    float uR[4], uUp[4], uDn[4];
+    if (nbk >= 0) {
+        uR[0] = r.x; uR[1] = r.y; uR[2] = r.z; uR[3] = r.w;
+        uUp[0] = uu.x; uUp[1] = uu.y; uUp[2] = uu.z; uUp[3] = uu.w;
+        uDn[0] = dd.x; uDn[1] = dd.y; uDn[2] = dd.z; uDn[3] = dd.w;
+    } else {
+        bc_ghost<float>(P, m, -nbk - 1, g, k, uL, nx, ny, t, uR);
+        hxR = hx_own;
+        for (int v = 0; v < 4; ++v) { uDn[v] = uL[v]; uUp[v] = uR[v]; }
+    }
+    float UpL[4], UpR[4];
+    if (P.limiter == LIM_VENKAT) {
+        const float K = (float)P.venkat_K;
+        const float KL = K * hx_own, KR = K * hxR;
+        const float e2L = KL * KL * KL, e2R = KR * KR * KR;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const float sc = 0.5f * (uL[v] * uL[v] + uR[v] * uR[v]);
+            UpL[v] = uL[v] + 0.5f * lim_venkat(uL[v] - uDn[v], uR[v] - uL[v], e2L * sc);
+            UpR[v] = uR[v] + 0.5f * lim_venkat(uR[v] - uUp[v], uL[v] - uR[v], e2R * sc);
+        }
+    } else {
+        const int lk = P.limiter;
+        const float ksi = (float)P.ksi;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            UpL[v] = uL[v] + 0.5f * limiter(lk, uL[v] - uDn[v], uR[v] - uL[v], ksi);
+            UpR[v] = uR[v] - 0.5f * limiter(lk, uR[v] - uL[v], uUp[v] - uR[v], ksi);
+        }
+    }
+    face_flux_fn<FLUX, float>(UpR, UpL, nx, ny, side, (float)P.gamma, g2, f);
+}
+
+__device__ __forceinline__ float4 avg4(const float4 &a, const float4 &b) {
+    return make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), 0.5f * (a.w + b.w));
+}
+
 // Diffusion source (calcDiffTerm.jl:88-113 and the extension models) in FP32.
 template <bool QUAD>
 __device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
@@ -144,12 +189,31 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
             const int4 dn = m.dn[g], up = m.up[g];
             int4 dn2 = make_int4(0, 0, 0, 0), up2 = make_int4(0, 0, 0, 0);
             if (QUAD && is_quad) { dn2 = m.dn2[g]; up2 = m.up2[g]; }
+            // every gather of faces 0-2 issued before any arithmetic (boundary
+            // faces load the cell itself and node 0, which they then ignore)
+            const int64_t Nc = m.Nc;
+            const float4 R0 = pin[nb.x >= 0 ? nb.x : g], R1 = pin[nb.y >= 0 ? nb.y : g], R2 = pin[nb.z >= 0 ? nb.z : g];
+            float4 D0 = nodeP[dn.x], D1 = nodeP[dn.y], D2 = nodeP[dn.z];
+            float4 W0 = nodeP[up.x], W1 = nodeP[up.y], W2 = nodeP[up.z];
+            const float nx0 = m.nxf[g], nx1 = m.nxf[Nc + g], nx2 = m.nxf[2 * Nc + g];
+            const float ny0 = m.nyf[g], ny1 = m.nyf[Nc + g], ny2 = m.nyf[2 * Nc + g];
+            const float l0 = m.lenf[g], l1 = m.lenf[Nc + g], l2 = m.lenf[2 * Nc + g];
+            float h0 = hx_own, h1 = hx_own, h2 = hx_own;
+            if (P.limiter == LIM_VENKAT) {
+                if (nb.x >= 0) h0 = m.hxf[nb.x];
+                if (nb.y >= 0) h1 = m.hxf[nb.y];
+                if (nb.z >= 0) h2 = m.hxf[nb.z];
+            }
+            if (QUAD && is_quad) {
+                D0 = avg4(D0, nodeP[dn2.x]); D1 = avg4(D1, nodeP[dn2.y]); D2 = avg4(D2, nodeP[dn2.z]);
+                W0 = avg4(W0, nodeP[up2.x]); W1 = avg4(W1, nodeP[up2.y]); W2 = avg4(W2, nodeP[up2.z]);
+            }
             float F[4], f[4];
-            face_flux_f<FLUX, QUAD>(m, P, pin, nodeP, g, 0, nb.x, dn.x, up.x, dn2.x, up2.x, is_quad, uL, hx_own, t, g2, F);
-            face_flux_f<FLUX, QUAD>(m, P, pin, nodeP, g, 1, nb.y, dn.y, up.y, dn2.y, up2.y, is_quad, uL, hx_own, t, g2, f);
+            face_flux_pre<FLUX>(m, P, g, 0, nb.x, R0, D0, W0, nx0, ny0, l0, uL, hx_own, h0, t, g2, F);
+            face_flux_pre<FLUX>(m, P, g, 1, nb.y, R1, D1, W1, nx1, ny1, l1, uL, hx_own, h1, t, g2, f);
 #pragma unroll
             for (int v = 0; v < 4; ++v) F[v] += f[v];
-            face_flux_f<FLUX, QUAD>(m, P, pin, nodeP, g, 2, nb.z, dn.z, up.z, dn2.z, up2.z, is_quad, uL, hx_own, t, g2, f);
+            face_flux_pre<FLUX>(m, P, g, 2, nb.z, R2, D2, W2, nx2, ny2, l2, uL, hx_own, h2, t, g2, f);
 #pragma unroll
             for (int v = 0; v < 4; ++v) F[v] += f[v];
             if (QUAD && is_quad) {
