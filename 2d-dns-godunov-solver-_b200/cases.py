@@ -132,6 +132,23 @@ def reference_tgv_case(n_nodes: int = 101, quads: bool = False):
     return mesh, cfg, (rho, u, v, p)
 
 
+def shard_cases(sizes, world: int, rank: int) -> List[int]:
+    """Indices of the independent cases rank `rank` of `world` advances:
+    greedy longest-processing-time assignment by cell count (largest case to
+    the least-loaded rank, ties to the lower rank), so every rank gets a
+    deterministic, nearly equal share with no data exchange between ranks."""
+    if world < 1 or not (0 <= rank < world):
+        raise ValueError("bad world/rank")
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i], i))
+    load = [0] * world
+    owner = [0] * len(sizes)
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += sizes[i]
+    return [i for i in range(len(sizes)) if owner[i] == rank]
+
+
 def batched_tgv(n_cases: int = 64, seed: int = 4, n_min: int = 64, n_max: int = 512) -> List[Tuple]:
     """Seeded TGV batch: nodes per side U{n_min..n_max}, Mach U(0.1,0.5), Re U(100,1600)."""
     rng = np.random.default_rng(seed)

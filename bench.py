@@ -154,6 +154,15 @@ def dist_max(dist, x):
     return float(t.item())
 
 
+def dist_sum(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def dist_barrier(dist):
     if dist is not None:
         dist.barrier()
@@ -239,8 +248,14 @@ def main():
     world, rank, local, dist = dist_setup(args)
     pkg = graft.load_package()
     items, desc, viscous = build_workload(pkg, args.config, args.precision)
+    sharded = world > 1 and len(items) > 1
+    if sharded:
+        # independent cases split across ranks (no data exchange), balanced by cells
+        mine = pkg.cases.shard_cases([m.nCells for m, _, _ in items], world, rank)
+        items = [items[i] for i in mine]
     metric = "Mcell-steps/s"
-    cfg_line = dict(desc, precision=args.precision, parallelism=("replicas%d" % world), l2_flush="inputs > L2")
+    cfg_line = dict(desc, precision=args.precision,
+                    parallelism=(("cases-sharded%d" if sharded else "replicas%d") % world), l2_flush="inputs > L2")
 
     if args.impl == "reference":
         if rank != 0:
@@ -273,7 +288,9 @@ def main():
     dist_barrier(dist)
     total_ms = dist_max(dist, total_ms)
     clocks = clk.summary()
-    value = cells * args.steps * world / (total_ms / 1e3) / 1e6
+    # whole-job cells: replicas each run the full mesh; shards add up
+    job_cells = dist_sum(dist, cells) if sharded else cells * world
+    value = job_cells * args.steps / (total_ms / 1e3) / 1e6
     ms_per_step = total_ms / args.steps
 
     # end to end through the C ABI with host buffers
