@@ -22,7 +22,7 @@ BC_KIND = {"inflow": 1, "outflow": 2, "slip": 3, "noslip_isothermal": 4, "tgv": 
 VISC = {"none": 0, "reference": 1, "sutherland": 2, "constant": 3}
 PRECISION = {"f64": 0, "mixed": 1}
 ORDER = {"natural": 0, "hilbert": 1, "rcm": 2}
-LOOP = {"cell": 0, "coloured": 1, "face": 2}
+LOOP = {"cell": 0, "coloured": 1, "face": 2, "tile": 3}
 
 EXPORTS = ("gd2d_abi_version", "gd2d_last_error", "gd2d_setup", "gd2d_set_state", "gd2d_set_conservative",
            "gd2d_propagate", "gd2d_get_history", "gd2d_get_state", "gd2d_calc_one_stage", "gd2d_update_variables",

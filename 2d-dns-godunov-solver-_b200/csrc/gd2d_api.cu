@@ -347,11 +347,25 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     }
     h->lc.block = block;
     h->lc.node_block = h->launch.node_block ? h->launch.node_block : 256;
+    if (h->lc.node_block != 64 && h->lc.node_block != 128 && h->lc.node_block != 256) {
+        delete h;
+        return fail(nullptr, GD2D_ERR_ARG, "node_block must be 64, 128 or 256");
+    }
     h->lc.persistent = h->launch.persistent;
-    h->lc.min_blocks = h->launch.min_blocks ? h->launch.min_blocks : 3;
+    // FP64 cell kernel: 3 blocks/SM (128 registers); mixed: 4 (fewer live values)
+    h->lc.min_blocks = h->launch.min_blocks ? h->launch.min_blocks : (h->mixed ? 4 : 3);
     if (h->lc.min_blocks < 2 || h->lc.min_blocks > 4) {
         delete h;
         return fail(nullptr, GD2D_ERR_ARG, "min_blocks must be 2, 3 or 4");
+    }
+    h->loop = h->launch.loop;
+    if (h->loop < GD2D_LOOP_CELL || h->loop > GD2D_LOOP_TILE_FACES) {
+        delete h;
+        return fail(nullptr, GD2D_ERR_ARG, "unknown loop variant %d", h->loop);
+    }
+    if (h->loop != GD2D_LOOP_CELL && h->loop != GD2D_LOOP_TILE_FACES && h->mixed) {
+        delete h;
+        return fail(nullptr, GD2D_ERR_ARG, "the face-loop variants run the FP64 path only");
     }
     h->graph_steps = h->launch.graph_steps > 0 ? h->launch.graph_steps : 32;
     h->flux = params[0].flux;
@@ -538,18 +552,9 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     // face list for the face-loop variants: each interior face once (from its
     // lower-indexed cell), boundary faces once; greedy edge colouring so that
     // no two faces of one colour share a cell
-    h->loop = h->launch.loop;
     std::vector<int4> faces;
-    if (h->loop != GD2D_LOOP_CELL) {
-        const char *bad = (h->loop != GD2D_LOOP_FACE_COLOURED && h->loop != GD2D_LOOP_FACE_SLOTS)
-                              ? "unknown loop variant"
-                              : (h->mixed ? "the face-loop variants run the FP64 path only" : nullptr);
-        if (bad) {
-            if (h->own_stream) cudaStreamDestroy(h->stream);
-            delete h;
-            return fail(nullptr, GD2D_ERR_ARG, "%s", bad);
-        }
-        auto code_k = [](const int4 &v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); };
+    auto code_k = [](const int4 &v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w)); };
+    if (h->loop == GD2D_LOOP_FACE_COLOURED || h->loop == GD2D_LOOP_FACE_SLOTS) {
         std::vector<uint8_t> used(Nc, 0);
         std::vector<int> colour;
         for (int64_t g = 0; g < Nc; ++g) {
@@ -580,6 +585,83 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         for (const int4 &f : faces) h->colour_off[f.w + 1]++;
         for (int c = 0; c < ncol; ++c) h->colour_off[c + 1] += h->colour_off[c];
         h->nfaces = (int64_t)faces.size();
+    }
+
+    // tile-local face lists: every face slot of a tile's cells, except that a
+    // face between two cells of the same tile is listed once (from the
+    // lower-indexed cell, its flux stored negated into the other cell's slot)
+    // when the other cell's evaluation of it is the exact negation: AUSM+
+    // with the Minmod or Venkatakrishnan limiter or none (the flux, the
+    // limiter and the role-aware epsilon are antisymmetric bit for bit),
+    // normals exactly negated, equal lengths, down/up nodes exchanged, both
+    // cells of the same kind and exactly one slot of each facing the other
+    std::vector<int64_t> tf_off;
+    std::vector<int4> tf_rec;
+    std::vector<int2> tf_q;
+    std::vector<double> tf_nx, tf_ny, tf_len;
+    if (h->loop == GD2D_LOOP_TILE_FACES) {
+        std::vector<char> case_pairs(n_cases, 0);
+        for (int c = 0; c < n_cases; ++c) {
+            const int lim = params[c].limiter;
+            case_pairs[c] = h->flux == GD2D_FLUX_AUSM_PLUS &&
+                            (lim == GD2D_LIM_NONE || lim == GD2D_LIM_MINMOD || lim == GD2D_LIM_VENKAT);
+        }
+        auto slot_facing = [&](int64_t b, int64_t a, int *count) {
+            int kb = -1;
+            *count = 0;
+            for (int q = 0; q < 4; ++q)
+                if (code_k(nbr[b], q) == (int)a) { kb = q; ++*count; }
+            return kb;
+        };
+        auto is_quad_cell = [&](int64_t g) { return h->quads && nbr[g].w != kAbsent; };
+        // (lo, klo) and (hi, khi): the two slots of one face, lo < hi
+        auto pairable = [&](int64_t lo, int klo, int64_t hi, int khi) {
+            if (!case_pairs[tile_case[lo / block]]) return false;
+            if (is_quad_cell(lo) != is_quad_cell(hi)) return false;
+            const size_t ol = (size_t)klo * Nc + lo, oh = (size_t)khi * Nc + hi;
+            if (!(gnx[oh] == -gnx[ol] && gny[oh] == -gny[ol] && glen[oh] == glen[ol])) return false;
+            if (code_k(dn[hi], khi) != code_k(up[lo], klo) || code_k(up[hi], khi) != code_k(dn[lo], klo)) return false;
+            if (is_quad_cell(lo) && (code_k(dn2[hi], khi) != code_k(up2[lo], klo) ||
+                                     code_k(up2[hi], khi) != code_k(dn2[lo], klo)))
+                return false;
+            return true;
+        };
+        tf_off.assign(ntiles + 1, 0);
+        for (int64_t t = 0; t < ntiles; ++t) {
+            for (int la = 0; la < block; ++la) {
+                const int64_t g = t * block + la;
+                const int4 nb = nbr[g];
+                if (nb.x == kAbsent) continue;
+                const bool quad = is_quad_cell(g);
+                const int nf = quad ? 4 : 3;
+                for (int k = 0; k < nf; ++k) {
+                    const int code = code_k(nb, k);
+                    int lbp = 0, kb = 0;
+                    if (code >= 0 && code != g && code / block == t) {
+                        int cb = 0, ca = 0;
+                        const int kk = slot_facing(code, g, &cb);
+                        slot_facing(g, code, &ca);
+                        if (kk >= 0 && cb == 1 && ca == 1) {
+                            const bool ok = (g < code) ? pairable(g, k, code, kk) : pairable(code, kk, g, k);
+                            if (ok) {
+                                if (code < g) continue;  // listed by the other cell
+                                lbp = (int)(code - t * block) + 1;
+                                kb = kk;
+                            }
+                        }
+                    }
+                    tf_rec.push_back(make_int4(code, pack_tile_face(la, k, lbp, kb, quad), code_k(dn[g], k),
+                                               code_k(up[g], k)));
+                    if (h->quads) tf_q.push_back(make_int2(code_k(dn2[g], k), code_k(up2[g], k)));
+                    const size_t o = (size_t)k * Nc + g;
+                    tf_nx.push_back(gnx[o]);
+                    tf_ny.push_back(gny[o]);
+                    tf_len.push_back(glen[o]);
+                }
+            }
+            tf_off[t + 1] = (int64_t)tf_rec.size();
+        }
+        h->nfaces = (int64_t)tf_rec.size();
     }
 
     // ------------------------------------------------------- device
@@ -663,7 +745,34 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         if (h->visc) { ALLOC(s.nodeCf, Nn); ALLOC(s.g1f, Nc); ALLOC(s.nodeGf, Nn); }
     }
     ALLOC(s.part, (size_t)ntiles * kPartials);
-    if (h->loop != GD2D_LOOP_CELL) {
+    if (h->loop == GD2D_LOOP_TILE_FACES) {
+        int64_t *d_tfo;
+        int4 *d_tfr;
+        int2 *d_tfq = nullptr;
+        double *d_tnx, *d_tny, *d_tlen;
+        ALLOC(d_tfo, tf_off.size()); UPLOAD(d_tfo, tf_off);
+        ALLOC(d_tfr, tf_rec.size()); UPLOAD(d_tfr, tf_rec);
+        if (h->quads) { ALLOC(d_tfq, tf_q.size()); UPLOAD(d_tfq, tf_q); }
+        if (!h->mixed) {
+            ALLOC(d_tnx, tf_nx.size()); UPLOAD(d_tnx, tf_nx);
+            ALLOC(d_tny, tf_ny.size()); UPLOAD(d_tny, tf_ny);
+            ALLOC(d_tlen, tf_len.size()); UPLOAD(d_tlen, tf_len);
+            m.tf_nx = d_tnx; m.tf_ny = d_tny; m.tf_len = d_tlen;
+        } else {
+            auto to_f = [](const std::vector<double> &v) {
+                std::vector<float> f(v.size());
+                for (size_t i = 0; i < v.size(); ++i) f[i] = (float)v[i];
+                return f;
+            };
+            float *f_nx, *f_ny, *f_len;
+            ALLOC(f_nx, tf_nx.size()); UPLOAD(f_nx, to_f(tf_nx));
+            ALLOC(f_ny, tf_ny.size()); UPLOAD(f_ny, to_f(tf_ny));
+            ALLOC(f_len, tf_len.size()); UPLOAD(f_len, to_f(tf_len));
+            m.tf_nxf = f_nx; m.tf_nyf = f_ny; m.tf_lenf = f_len;
+        }
+        m.tf_off = d_tfo; m.tf_rec = d_tfr; m.tf_q = d_tfq;
+    }
+    if (h->loop == GD2D_LOOP_FACE_COLOURED || h->loop == GD2D_LOOP_FACE_SLOTS) {
         ALLOC(h->d_faces, faces.size()); UPLOAD(h->d_faces, faces);
         if (h->loop == GD2D_LOOP_FACE_COLOURED) ALLOC(h->Facc, Nc);
         else ALLOC(h->Fslot, (size_t)nfmax * Nc);
@@ -812,6 +921,9 @@ static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, 
             if (e != cudaSuccess) return e;
         }
         e = launch_face_update_f64(h->m, h->s, h->visc, h->quads, false, h->Facc, nullptr, h->lc, h->stream);
+    } else if (h->loop == GD2D_LOOP_TILE_FACES) {
+        e = h->mixed ? launch_cell_step_tf_mixed(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream)
+                     : launch_cell_step_tf_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream);
     } else if (h->loop == GD2D_LOOP_FACE_SLOTS) {
         e = launch_face_flux_f64(h->m, h->s, h->flux, h->quads, true, h->d_faces, 0, h->nfaces, nullptr, h->Fslot,
                                  h->lc, h->stream);
@@ -1083,9 +1195,167 @@ int gd2d_calc_diff_term(gd2d_handle *h, int32_t icase, double *diff) {
     h->split_diff_valid = true;
     return download_cells(h, icase, h->split_diff, diff);
 }
-int gd2d_autotune(gd2d_handle *h, int32_t, gd2d_launch *) {
+// ------------------------------------------------------------ autotuner
+
+namespace {
+
+struct Region {
+    void *p;
+    size_t bytes;
+};
+
+// Every device array a step reads before writing or leaves behind for the
+// next step: saving and restoring these makes trial steps invisible.
+std::vector<Region> step_state(const gd2d_handle *h) {
+    const DevState &s = h->s;
+    const DevMesh &m = h->m;
+    std::vector<Region> r;
+    auto add = [&](const void *p, size_t b) {
+        if (p && b) r.push_back({const_cast<void *>(p), b});
+    };
+    add(s.U, sizeof(double4) * m.Nc);
+    add(s.prim, sizeof(double4) * 2 * m.Nc);
+    add(s.nodeP, sizeof(double4) * m.Nn);
+    add(s.nodeC, sizeof(double4) * m.Nn);
+    add(s.g1, sizeof(NodeGrad) * m.Nc);
+    add(s.nodeG, sizeof(NodeGrad) * m.Nn);
+    add(s.primf, sizeof(float4) * 2 * m.Nc);
+    add(s.nodePf, sizeof(float4) * m.Nn);
+    add(s.nodeCf, sizeof(float4) * m.Nn);
+    add(s.g1f, sizeof(NodeGradF) * m.Nc);
+    add(s.nodeGf, sizeof(NodeGradF) * m.Nn);
+    add(s.part, sizeof(double) * m.ntiles * kPartials);
+    add(s.cstate, sizeof(CaseState) * m.ncases);
+    add(s.ring, sizeof(DevStats) * s.ring_len * m.ncases);
+    add(s.parity, sizeof(int32_t));
+    add(s.node_done, sizeof(unsigned int));
+    add(h->Facc, sizeof(double4) * m.Nc);
+    add(h->Fslot, sizeof(double4) * m.nfmax * m.Nc);
+    return r;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+cudaError_t copy_regions(const std::vector<Region> &reg, char *snap, bool save, cudaStream_t st) {
+    size_t off = 0;
+    for (const Region &r : reg) {
+        cudaError_t e = save ? cudaMemcpyAsync(snap + off, r.p, r.bytes, cudaMemcpyDeviceToDevice, st)
+                             : cudaMemcpyAsync(r.p, snap + off, r.bytes, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
+        off += align256(r.bytes);
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+// Device time per step of the handle's current launch shape: restore the
+// saved state, one untimed graph (warm-up), restore, then `reps` timed graphs.
+static int time_shape(gd2d_handle *h, const std::vector<Region> &reg, char *snap, int reps, double *ms_per_step) {
+    const int G = h->graph_steps;
+    int rc = G > 1 ? capture_graph(h, G, false) : (drop_graph(h), GD2D_OK);
+    if (rc) return rc;
+    auto run = [&](int n) -> cudaError_t {
+        for (int q = 0; q < n; ++q) {
+            cudaError_t e = G > 1 ? cudaGraphLaunch(h->graph, h->stream) : launch_step_kernels(h, nullptr, nullptr);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    };
+    CUDA_TRY(h, copy_regions(reg, snap, false, h->stream));
+    CUDA_TRY(h, run(1));
+    CUDA_TRY(h, copy_regions(reg, snap, false, h->stream));
+    CUDA_TRY(h, cudaEventRecord(h->ev_total[0], h->stream));
+    CUDA_TRY(h, run(reps));
+    CUDA_TRY(h, cudaEventRecord(h->ev_total[1], h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    CUDA_TRY(h, cudaEventElapsedTime(&ms, h->ev_total[0], h->ev_total[1]));
+    *ms_per_step = (double)ms / ((double)reps * G);
+    return GD2D_OK;
+}
+
+int gd2d_autotune(gd2d_handle *h, int32_t steps_per_trial, gd2d_launch *chosen) {
     if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");
-    return fail(h, GD2D_ERR_STATE, "gd2d_autotune: not built yet");
+    if (!h->state_ready) return fail(h, GD2D_ERR_STATE, "gd2d_set_state must be called for every case first");
+    if (steps_per_trial <= 0) steps_per_trial = 64;
+    cudaSetDevice(h->device);
+    const std::vector<Region> reg = step_state(h);
+    size_t total = 0;
+    for (const Region &r : reg) total += align256(r.bytes);
+    char *snap = nullptr;
+    {
+        cudaError_t e = cudaMalloc((void **)&snap, total);
+        if (e != cudaSuccess) return fail(h, GD2D_ERR_OOM, "autotune snapshot of %zu bytes: %s", total,
+                                          cudaGetErrorString(e));
+    }
+    CUDA_TRY(h, copy_regions(reg, snap, true, h->stream));
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
+    const LaunchCfg lc0 = h->lc;
+    const int G0 = h->graph_steps;
+    auto set_shape = [&](const LaunchCfg &lc, int G) {
+        h->lc = lc;
+        h->lc.grid = dev_sms * lc.min_blocks * (256 / lc.block);
+        h->graph_steps = G;
+    };
+    auto trial = [&](const LaunchCfg &lc, int G, double *ms) {
+        set_shape(lc, G);
+        const int reps = std::max(1, (steps_per_trial + G - 1) / G);
+        return time_shape(h, reg, snap, reps, ms);
+    };
+    LaunchCfg best = lc0;
+    int bestG = G0;
+    double best_ms = 0.0;
+    int rc = trial(best, bestG, &best_ms);
+    // coordinate search: register budget x persistence, then node-pass block,
+    // then steps per graph
+    for (int mb = 2; rc == GD2D_OK && mb <= 4; ++mb) {
+        for (int pers = 0; rc == GD2D_OK && pers <= 1; ++pers) {
+            LaunchCfg c = best;
+            c.min_blocks = mb;
+            c.persistent = pers;
+            if (c.min_blocks == best.min_blocks && c.persistent == best.persistent) continue;
+            double ms = 0.0;
+            rc = trial(c, bestG, &ms);
+            if (rc == GD2D_OK && ms < best_ms) { best = c; best_ms = ms; }
+        }
+    }
+    for (int nb : {64, 128, 256}) {
+        if (rc != GD2D_OK || nb == best.node_block) continue;
+        LaunchCfg c = best;
+        c.node_block = nb;
+        double ms = 0.0;
+        rc = trial(c, bestG, &ms);
+        if (rc == GD2D_OK && ms < best_ms) { best = c; best_ms = ms; }
+    }
+    for (int G : {8, 32, 128}) {
+        if (rc != GD2D_OK || G == bestG || G > h->s.ring_len) continue;
+        double ms = 0.0;
+        rc = trial(best, G, &ms);
+        if (rc == GD2D_OK && ms < best_ms) { bestG = G; best_ms = ms; }
+    }
+    // put the state back whatever happened; on failure keep the old shape
+    drop_graph(h);
+    cudaError_t e = copy_regions(reg, snap, false, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(snap);
+    if (rc != GD2D_OK) {
+        set_shape(lc0, G0);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        set_shape(lc0, G0);
+        return fail(h, GD2D_ERR_CUDA, "autotune restore: %s", cudaGetErrorString(e));
+    }
+    set_shape(best, bestG);
+    h->launch.min_blocks = best.min_blocks;
+    h->launch.persistent = best.persistent;
+    h->launch.node_block = best.node_block;
+    h->launch.graph_steps = bestG;
+    h->last_total_ms = best_ms;
+    if (chosen) *chosen = h->launch;
+    return GD2D_OK;
 }
 
 int gd2d_last_timing(gd2d_handle *h, double *total_ms, double *cell_kernel_ms, int64_t *launches) {

@@ -98,7 +98,35 @@ struct DevMesh {
     // mixed precision: FP32 copies of the geometry (the FP64 planes are not allocated)
     const float *nxf, *nyf, *lenf;       // [nfmax][Nc]
     const float *rareaf, *areaf, *hxf, *charlenf;
+    // tile-local face lists (GD2D_LOOP_TILE_FACES): faces of tile t are
+    // [tf_off[t], tf_off[t+1]); tf_rec = (neighbour code, packed slots, dn, up)
+    // with packed = la | ka << 10 | (lb + 1) << 12 | kb << 22 | quad << 24
+    // (lb + 1 = 0: the face is not shared with another cell of the tile);
+    // tf_q = (dn2, up2) for quads; the face geometry of slot (la, ka)
+    const int64_t *tf_off;               // [ntiles + 1]
+    const int4 *tf_rec;
+    const int2 *tf_q;
+    const double *tf_nx, *tf_ny, *tf_len;
+    const float *tf_nxf, *tf_nyf, *tf_lenf;
 };
+
+// Fields of a packed tile-face slot record.
+struct TileFace {
+    int la, ka, lbp, kb;
+    bool quad;
+};
+__host__ __device__ __forceinline__ TileFace unpack_tile_face(int32_t w) {
+    TileFace f;
+    f.la = w & 1023;
+    f.ka = (w >> 10) & 3;
+    f.lbp = (w >> 12) & 1023;
+    f.kb = (w >> 22) & 3;
+    f.quad = ((w >> 24) & 1) != 0;
+    return f;
+}
+__host__ __device__ __forceinline__ int32_t pack_tile_face(int la, int ka, int lbp, int kb, bool quad) {
+    return (int32_t)(la | (ka << 10) | (lbp << 12) | (kb << 22) | ((quad ? 1 : 0) << 24));
+}
 
 struct NodeGradF {  // FP32 node means of the first gradients
     float2 ru, rv, re;
@@ -140,6 +168,8 @@ void set_handleless_error(const char *msg);
 // Launchers implemented in kernels_f64.cu.
 cudaError_t launch_cell_step_f64(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
                                  const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_cell_step_tf_f64(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
+                                    const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, bool flip_parity,
                                 bool zero_prims, int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);
@@ -167,6 +197,8 @@ cudaError_t launch_diff_only_f64(const DevMesh &m, const DevState &s, double4 *d
 // viscous terms; FP64 state update and reductions).
 cudaError_t launch_cell_step_mixed(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
                                    const LaunchCfg &lc, cudaStream_t st);
+cudaError_t launch_cell_step_tf_mixed(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
+                                      const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_node_avg_mixed(const DevMesh &m, const DevState &s, bool visc, bool flip_parity,
                                   bool zero_prims, int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_visc_grad_mixed(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);

@@ -6,163 +6,11 @@
 // packed as float4 so each neighbour or node gather is one 128-bit load.
 // Built with fast FP32 division and square root; the error of this path is
 // reported against the FP64 oracle rather than asserted bit-exact.
-#include "step_kernels.cuh"
+#include "mixed_face.cuh"
 
 namespace gd2d {
 
 namespace {
-
-// computeInterfaceSlope (computeslope2d.jl:3-136) in FP32.
-template <int FLUX, bool QUAD>
-__device__ __forceinline__ void face_flux_f(const DevMesh &m, const DevCase &P, const float4 *__restrict__ pin,
-                                            const float4 *__restrict__ nodeP, int64_t g, int k, int nbk, int dnk,
-                                            int upk, int dn2k, int up2k, bool is_quad, const float *uL, float hx_own,
-                                            double t, float g2, float *f) {
-    const int64_t o = (int64_t)k * m.Nc + g;
-    const float side = m.lenf[o], nx = m.nxf[o], ny = m.nyf[o];
-    float uR[4], uUp[4], uDn[4];
-    float hxR = hx_own;
-    if (nbk >= 0) {
-        if (QUAD && is_quad) {
-            float4 a = nodeP[upk], a2 = nodeP[up2k], b = nodeP[dnk], b2 = nodeP[dn2k];
-            uUp[0] = 0.5f * (a.x + a2.x); uUp[1] = 0.5f * (a.y + a2.y);
-            uUp[2] = 0.5f * (a.z + a2.z); uUp[3] = 0.5f * (a.w + a2.w);
-            uDn[0] = 0.5f * (b.x + b2.x); uDn[1] = 0.5f * (b.y + b2.y);
-            uDn[2] = 0.5f * (b.z + b2.z); uDn[3] = 0.5f * (b.w + b2.w);
-        } else {
-            float4 a = nodeP[upk], b = nodeP[dnk];
-            uUp[0] = a.x; uUp[1] = a.y; uUp[2] = a.z; uUp[3] = a.w;
-            uDn[0] = b.x; uDn[1] = b.y; uDn[2] = b.z; uDn[3] = b.w;
-        }
-        float4 r = pin[nbk];
-        uR[0] = r.x; uR[1] = r.y; uR[2] = r.z; uR[3] = r.w;
-        if (P.limiter == LIM_VENKAT) hxR = m.hxf[nbk];
-    } else {
-        bc_ghost<float>(P, m, -nbk - 1, g, k, uL, nx, ny, t, uR);
-        for (int v = 0; v < 4; ++v) { uDn[v] = uL[v]; uUp[v] = uR[v]; }
-    }
-    float UpL[4], UpR[4];
-    if (P.limiter == LIM_VENKAT) {
-        const float K = (float)P.venkat_K;
-        const float KL = K * hx_own, KR = K * hxR;
-        const float e2L = KL * KL * KL, e2R = KR * KR * KR;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const float sc = 0.5f * (uL[v] * uL[v] + uR[v] * uR[v]);
-            UpL[v] = uL[v] + 0.5f * lim_venkat(uL[v] - uDn[v], uR[v] - uL[v], e2L * sc);
-            UpR[v] = uR[v] + 0.5f * lim_venkat(uR[v] - uUp[v], uL[v] - uR[v], e2R * sc);
-        }
-    } else {
-        const int lk = P.limiter;
-        const float ksi = (float)P.ksi;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            UpL[v] = uL[v] + 0.5f * limiter(lk, uL[v] - uDn[v], uR[v] - uL[v], ksi);
-            UpR[v] = uR[v] - 0.5f * limiter(lk, uR[v] - uL[v], uUp[v] - uR[v], ksi);
-        }
-    }
-    face_flux_fn<FLUX, float>(UpR, UpL, nx, ny, side, (float)P.gamma, g2, f);
-}
-
-// The same face with every gathered input already in registers: r = the
-// neighbour's primitives, d/u = down/up node primitives (quads: averaged),
-// geometry (nx, ny, side).  Boundary faces ignore r, d, u.
-template <int FLUX>
-__device__ __forceinline__ void face_flux_pre(const DevMesh &m, const DevCase &P, int64_t g, int k, int nbk,
-                                              const float4 &r, const float4 &dd, const float4 &uu, float nx, float ny,
-                                              float side, const float *uL, float hx_own, float hxR, double t, float g2,
-                                              float *f) {
-    float uR[4], uUp[4], uDn[4];
-    if (nbk >= 0) {
-        uR[0] = r.x; uR[1] = r.y; uR[2] = r.z; uR[3] = r.w;
-        uUp[0] = uu.x; uUp[1] = uu.y; uUp[2] = uu.z; uUp[3] = uu.w;
-        uDn[0] = dd.x; uDn[1] = dd.y; uDn[2] = dd.z; uDn[3] = dd.w;
-    } else {
-        bc_ghost<float>(P, m, -nbk - 1, g, k, uL, nx, ny, t, uR);
-        hxR = hx_own;
-        for (int v = 0; v < 4; ++v) { uDn[v] = uL[v]; uUp[v] = uR[v]; }
-    }
-    float UpL[4], UpR[4];
-    if (P.limiter == LIM_VENKAT) {
-        const float K = (float)P.venkat_K;
-        const float KL = K * hx_own, KR = K * hxR;
-        const float e2L = KL * KL * KL, e2R = KR * KR * KR;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const float sc = 0.5f * (uL[v] * uL[v] + uR[v] * uR[v]);
-            UpL[v] = uL[v] + 0.5f * lim_venkat(uL[v] - uDn[v], uR[v] - uL[v], e2L * sc);
-            UpR[v] = uR[v] + 0.5f * lim_venkat(uR[v] - uUp[v], uL[v] - uR[v], e2R * sc);
-        }
-    } else {
-        const int lk = P.limiter;
-        const float ksi = (float)P.ksi;
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            UpL[v] = uL[v] + 0.5f * limiter(lk, uL[v] - uDn[v], uR[v] - uL[v], ksi);
-            UpR[v] = uR[v] - 0.5f * limiter(lk, uR[v] - uL[v], uUp[v] - uR[v], ksi);
-        }
-    }
-    face_flux_fn<FLUX, float>(UpR, UpL, nx, ny, side, (float)P.gamma, g2, f);
-}
-
-__device__ __forceinline__ float4 avg4(const float4 &a, const float4 &b) {
-    return make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), 0.5f * (a.w + b.w));
-}
-
-// Diffusion source (calcDiffTerm.jl:88-113 and the extension models) in FP32.
-template <bool QUAD>
-__device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
-                                              bool is_quad, const float4 &me, float *diff) {
-    const int nf = (QUAD && is_quad) ? 4 : 3;
-    float sx[3] = {0.f, 0.f, 0.f}, sy[3] = {0.f, 0.f, 0.f};
-    float du = 0.f, dv = 0.f;
-    const bool art = (P.visc_model != VISC_REFERENCE) && P.art_visc;
-    for (int k = 0; k < nf; ++k) {
-        const int64_t o = (int64_t)k * m.Nc + g;
-        const float side = m.lenf[o], nx = m.nxf[o], ny = m.nyf[o];
-        const int2 e = m.c2n[o];
-        const NodeGradF A = s.nodeGf[e.x], B = s.nodeGf[e.y];
-        sx[0] += 0.5f * (A.ru.x + B.ru.x) * -ny * side; sy[0] += 0.5f * (A.ru.y + B.ru.y) * -nx * side;
-        sx[1] += 0.5f * (A.rv.x + B.rv.x) * -ny * side; sy[1] += 0.5f * (A.rv.y + B.rv.y) * -nx * side;
-        sx[2] += 0.5f * (A.re.x + B.re.x) * -ny * side; sy[2] += 0.5f * (A.re.y + B.re.y) * -nx * side;
-        if (art) {
-            const float4 na = s.nodePf[e.x], nb = s.nodePf[e.y];
-            du += 0.5f * (na.y + nb.y) * -nx * side;
-            dv += 0.5f * (na.z + nb.z) * -ny * side;
-        }
-    }
-    const float rA = m.rareaf[g];
-    float lap[3];
-#pragma unroll
-    for (int v = 0; v < 3; ++v) lap[v] = (sx[v] + sy[v]) * rA;
-    const float T = me.w / me.x / (float)P.R;
-    diff[0] = 0.f;
-    if (P.visc_model == VISC_REFERENCE) {
-        const float mu = (float)P.mu_ref;
-        diff[1] = mu * lap[0];
-        diff[2] = mu * lap[1];
-        diff[3] = mu * (float)air_conductivity((double)T) * lap[2];
-    } else {
-        const float mu = (P.visc_model == VISC_SUTHERLAND)
-                             ? (float)P.mu_ref * (sutherland(T) / (float)P.suth_ref)
-                             : (float)P.mu_ref;
-        float mart = 0.f;
-        if (art) {
-            const float HX = m.hxf[g];
-            const float divU = (du + dv) * rA;
-            const float aS = sqrtf((float)P.gamma * me.w / me.x);
-            const float a = 0.05f * aS / HX * 0.70710678f;
-            if (-divU > a) {
-                const float tmp = divU * divU - a * a;
-                if (tmp > 0.f) mart = 0.5f * me.x * (HX * HX * 0.5f) * sqrtf(tmp) * 1.0e-5f;
-            }
-        }
-        const float mue = mu + mart;
-        diff[1] = mue * lap[0];
-        diff[2] = mue * lap[1];
-        diff[3] = mue * lap[2];
-    }
-}
 
 template <int FLUX, bool VISC, bool QUAD, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, const DevState s) {
@@ -223,43 +71,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
             }
             float diff[4] = {0.f, 0.f, 0.f, 0.f};
             if (VISC) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
-            // FP32 increment, FP64 accumulation of the Euler update
-            const float bdt = (float)(P.beta * dt);
-            const float rarea = m.rareaf[g];
-            const double4 U = s.U[g];
-            const double Uo[4] = {U.x, U.y, U.z, U.w};
-            double Un[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) Un[v] = Uo[v] + (double)(bdt * (diff[v] - F[v] * rarea));
-            if (P.density_constrained == 1) {
-                if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
-                if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
-            }
-            s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
-            // primitives from the FP64 state
-            const double rho = Un[0];
-            const double rinv = 1.0 / rho;
-            const double ux = Un[1] * rinv;
-            const double uy = Un[2] * rinv;
-            const double p = (P.gamma - 1.0) * (Un[3] - 0.5 * (Un[1] * ux + Un[2] * uy));
-            const float a = sqrtf((float)(P.gamma * p * rinv));
-            const float vmax = sqrtf((float)(ux * ux + uy * uy)) + a;
-            pout[g] = make_float4((float)rho, (float)ux, (float)uy, (float)p);
-            const double area = (double)m.areaf[g];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const double d = Un[v] - Uo[v];
-                part.res[v] = d * d;
-                part.tot[v] = Un[v] * area;
-            }
-            part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
-            part.vmax = (double)vmax;
-            part.rmin = (double)(m.charlenf[g] / vmax);
-            part.rhomin = (double)me.x;
-            part.rhomax = (double)me.x;
-            const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
-                            (p > 0.0);
-            part.bad = ok ? 0.0 : 1.0;
+            cell_update_mixed(m, s, P, g, me, F, diff, dt, pout, part);
         }
         tile_epilogue(m, s, tile, c, part, sh, false);
     }

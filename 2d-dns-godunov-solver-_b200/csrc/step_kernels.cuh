@@ -147,16 +147,16 @@ __device__ __forceinline__ void tile_epilogue(const DevMesh &m, const DevState &
 
 // --------------------------------------------------------- MUSCL + flux
 
-// computeInterfaceSlope, computeslope2d.jl:3-136, for face k of cell g.
+// computeInterfaceSlope, computeslope2d.jl:3-136, for face k of cell g with
+// its operands already fetched: neighbour code nbk (cell id or -(bc slot+1)),
+// the neighbour's primitives r and HX (interior faces), the face geometry.
 template <int FLUX, bool QUAD>
-__device__ __forceinline__ void face_flux(const DevMesh &m, const DevCase &P, const double4 *__restrict__ pin,
-                                          const double4 *__restrict__ nodeP, int64_t g, int k, int nbk,
-                                          int dnk, int upk, int dn2k, int up2k, bool is_quad, const double *uL,
-                                          double hx_own, double t, double g2, double *f) {
-    const int64_t o = (int64_t)k * m.Nc + g;
-    const double side = m.len[o], nx = m.nx[o], ny = m.ny[o];
+__device__ __forceinline__ void face_flux_at(const DevMesh &m, const DevCase &P, const double4 *__restrict__ nodeP,
+                                             int64_t g, int k, int nbk, int dnk, int upk, int dn2k, int up2k,
+                                             bool is_quad, const double *uL, const double4 &r, double hx_own,
+                                             double hxR, double side, double nx, double ny, double t, double g2,
+                                             double *f) {
     double uR[4], uUp[4], uDn[4];
-    double hxR = hx_own;
     if (nbk >= 0) {
         if (QUAD && is_quad) {
             double4 a = nodeP[upk], a2 = nodeP[up2k], b = nodeP[dnk], b2 = nodeP[dn2k];
@@ -169,12 +169,11 @@ __device__ __forceinline__ void face_flux(const DevMesh &m, const DevCase &P, co
             uUp[0] = a.x; uUp[1] = a.y; uUp[2] = a.z; uUp[3] = a.w;
             uDn[0] = b.x; uDn[1] = b.y; uDn[2] = b.z; uDn[3] = b.w;
         }
-        double4 r = pin[nbk];
         uR[0] = r.x; uR[1] = r.y; uR[2] = r.z; uR[3] = r.w;
-        if (P.limiter == LIM_VENKAT) hxR = m.hx[nbk];
     } else {
         bc_ghost<double>(P, m, -nbk - 1, g, k, uL, nx, ny, t, uR);
         for (int v = 0; v < 4; ++v) { uDn[v] = uL[v]; uUp[v] = uR[v]; }
+        hxR = hx_own;
     }
     double UpL[4], UpR[4];
     if (P.limiter == LIM_VENKAT) {
@@ -197,6 +196,24 @@ __device__ __forceinline__ void face_flux(const DevMesh &m, const DevCase &P, co
         }
     }
     face_flux_fn<FLUX, double>(UpR, UpL, nx, ny, side, P.gamma, g2, f);
+}
+
+// Face k of cell g, fetching its operands from the per-cell arrays.
+template <int FLUX, bool QUAD>
+__device__ __forceinline__ void face_flux(const DevMesh &m, const DevCase &P, const double4 *__restrict__ pin,
+                                          const double4 *__restrict__ nodeP, int64_t g, int k, int nbk,
+                                          int dnk, int upk, int dn2k, int up2k, bool is_quad, const double *uL,
+                                          double hx_own, double t, double g2, double *f) {
+    const int64_t o = (int64_t)k * m.Nc + g;
+    const double side = m.len[o], nx = m.nx[o], ny = m.ny[o];
+    double4 r = make_double4(0.0, 0.0, 0.0, 0.0);
+    double hxR = hx_own;
+    if (nbk >= 0) {
+        r = pin[nbk];
+        if (P.limiter == LIM_VENKAT) hxR = m.hx[nbk];
+    }
+    face_flux_at<FLUX, QUAD>(m, P, nodeP, g, k, nbk, dnk, upk, dn2k, up2k, is_quad, uL, r, hx_own, hxR, side, nx, ny,
+                             t, g2, f);
 }
 
 // Second Green-Gauss pass and transport model: the diffusion source of
@@ -261,6 +278,48 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
     }
 }
 
+// Euler update (calcOneStageMUSCLcpuFast.jl:94-99), the densityConstrained
+// clamp (evaluate2d.jl:63-77), updateVariablesSA (evaluate2d.jl:87-104) and
+// the cell's contribution to the step's reductions.
+__device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
+                                            const double4 &me, const double *F, const double *diff, double dt,
+                                            double4 *__restrict__ pout, Part &part) {
+    const double rarea = m.rarea[g];
+    const double4 U = s.U[g];
+    const double Uo[4] = {U.x, U.y, U.z, U.w};
+    double Un[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) Un[v] = (Uo[v] - F[v] * P.beta * dt * rarea + P.beta * dt * diff[v]);
+    if (P.density_constrained == 1) {
+        if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
+        if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
+    }
+    s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
+    const double gam = P.gamma;
+    const double rho = Un[0];
+    const double ux = Un[1] / Un[0];
+    const double uy = Un[2] / Un[0];
+    const double p = (gam - 1.0) * (Un[3] - 0.5 * (Un[1] * Un[1] + Un[2] * Un[2]) / Un[0]);
+    const double a = sqrt(gam * p / rho);
+    const double vmax = sqrt(ux * ux + uy * uy) + a;
+    pout[g] = make_double4(rho, ux, uy, p);
+    const double area = m.area[g];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const double d = Un[v] - Uo[v];
+        part.res[v] = d * d;
+        part.tot[v] = Un[v] * area;
+    }
+    part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
+    part.vmax = vmax;
+    part.rmin = m.charlen[g] / vmax;
+    part.rhomin = me.x;
+    part.rhomax = me.x;
+    const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
+                    (p > 0.0);
+    part.bad = ok ? 0.0 : 1.0;
+}
+
 // ---------------------------------------------------- fused cell kernel
 
 template <int FLUX, bool VISC, bool QUAD, int MINB>
@@ -303,41 +362,91 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const 
             }
             double diff[4] = {0.0, 0.0, 0.0, 0.0};
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
-            // Euler update, calcOneStageMUSCLcpuFast.jl:94-99
-            const double rarea = m.rarea[g];
-            const double4 U = s.U[g];
-            const double Uo[4] = {U.x, U.y, U.z, U.w};
-            double Un[4];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) Un[v] = (Uo[v] - F[v] * P.beta * dt * rarea + P.beta * dt * diff[v]);
-            if (P.density_constrained == 1) {  // evaluate2d.jl:63-77
-                if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
-                if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
+            cell_update(m, s, P, g, me, F, diff, dt, pout, part);
+        }
+        tile_epilogue(m, s, tile, c, part, sh, false);
+    }
+}
+
+// The fused cell kernel over tile-local face lists (GD2D_LOOP_TILE_FACES).
+// Phase 1 stages the tile's primitives (and HX) in shared memory; phase 2
+// runs the tile's face list, one face per thread: a face between two cells
+// of the tile is computed once, from its lower-indexed cell, and its flux
+// stored negated into the other cell's slot -- exact because the listed
+// pairs are only those whose face state and flux are antisymmetric bit for
+// bit under exchange of the two cells (checked on the host: AUSM+ with the
+// Minmod or Venkatakrishnan limiter or none, negated normals, exchanged
+// down/up nodes); every other face slot is computed from its own cell as in
+// k_cell_step.  Phase 3 sums each cell's slots in face order
+// (calcOneStageMUSCLcpuFast.jl:66-85) and finishes the cell as k_cell_step.
+template <int FLUX, bool VISC, bool QUAD, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, const DevState s) {
+    constexpr int NS = QUAD ? 4 : 3;
+    __shared__ Part sh[8];
+    __shared__ double4 s_prim[256];
+    __shared__ double s_hx[256];
+    __shared__ double4 s_flux[NS][256];
+    const int par = *s.parity;
+    const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
+    double4 *__restrict__ pout = s.prim + (int64_t)(par ^ 1) * m.Nc;
+    const int B = blockDim.x;
+    for (int64_t tile = blockIdx.x; tile < m.ntiles; tile += gridDim.x) {
+        const int c = m.tile_case[tile];
+        const DevCase &P = m.cases[c];
+        const double dt = s.cstate[c].dt, t = s.cstate[c].t;
+        const int64_t base = tile * B;
+        const int64_t g = base + threadIdx.x;
+        const bool venkat = P.limiter == LIM_VENKAT;
+        const double4 me = pin[g];
+        s_prim[threadIdx.x] = me;
+        if (venkat) s_hx[threadIdx.x] = m.hx[g];
+        __syncthreads();
+        const double gam = P.gamma;
+        const double g2 = 2.0 * (gam - 1.0) / (gam + 1.0);
+        const int64_t f1 = m.tf_off[tile + 1];
+        for (int64_t f = m.tf_off[tile] + threadIdx.x; f < f1; f += B) {
+            const int4 rec = m.tf_rec[f];
+            const TileFace tf = unpack_tile_face(rec.y);
+            const double4 a4 = s_prim[tf.la];
+            const double uL[4] = {a4.x, a4.y, a4.z, a4.w};
+            const double hx_own = venkat ? s_hx[tf.la] : 0.0;
+            double4 r = make_double4(0.0, 0.0, 0.0, 0.0);
+            double hxR = hx_own;
+            if (rec.x >= 0) {
+                const int64_t lr = (int64_t)rec.x - base;
+                if (lr >= 0 && lr < B) {
+                    r = s_prim[lr];
+                    if (venkat) hxR = s_hx[lr];
+                } else {
+                    r = pin[rec.x];
+                    if (venkat) hxR = m.hx[rec.x];
+                }
             }
-            s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
-            // updateVariablesSA, evaluate2d.jl:87-104
-            const double rho = Un[0];
-            const double ux = Un[1] / Un[0];
-            const double uy = Un[2] / Un[0];
-            const double p = (gam - 1.0) * (Un[3] - 0.5 * (Un[1] * Un[1] + Un[2] * Un[2]) / Un[0]);
-            const double a = sqrt(gam * p / rho);
-            const double vmax = sqrt(ux * ux + uy * uy) + a;
-            pout[g] = make_double4(rho, ux, uy, p);
-            const double area = m.area[g];
-#pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                const double d = Un[v] - Uo[v];
-                part.res[v] = d * d;
-                part.tot[v] = Un[v] * area;
+            int2 q2 = make_int2(0, 0);
+            if (QUAD && tf.quad) q2 = m.tf_q[f];
+            double fv[4];
+            face_flux_at<FLUX, QUAD>(m, P, s.nodeP, base + tf.la, tf.ka, rec.x, rec.z, rec.w, q2.x, q2.y,
+                                     QUAD && tf.quad, uL, r, hx_own, hxR, m.tf_len[f], m.tf_nx[f], m.tf_ny[f], t,
+                                     g2, fv);
+            s_flux[tf.ka][tf.la] = make_double4(fv[0], fv[1], fv[2], fv[3]);
+            if (tf.lbp) s_flux[tf.kb][tf.lbp - 1] = make_double4(-fv[0], -fv[1], -fv[2], -fv[3]);
+        }
+        __syncthreads();
+        Part part;
+        part.init();
+        const int4 nb = m.nbr[g];
+        if (nb.x != kAbsent) {
+            const bool is_quad = QUAD && (nb.w != kAbsent);
+            const double4 a0 = s_flux[0][threadIdx.x], a1 = s_flux[1][threadIdx.x], a2 = s_flux[2][threadIdx.x];
+            double F[4] = {a0.x + a1.x, a0.y + a1.y, a0.z + a1.z, a0.w + a1.w};
+            F[0] = F[0] + a2.x; F[1] = F[1] + a2.y; F[2] = F[2] + a2.z; F[3] = F[3] + a2.w;
+            if (QUAD && is_quad) {
+                const double4 a3 = s_flux[NS - 1][threadIdx.x];
+                F[0] = F[0] + a3.x; F[1] = F[1] + a3.y; F[2] = F[2] + a3.z; F[3] = F[3] + a3.w;
             }
-            part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
-            part.vmax = vmax;
-            part.rmin = m.charlen[g] / vmax;
-            part.rhomin = me.x;
-            part.rhomax = me.x;
-            const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
-                            (p > 0.0);
-            part.bad = ok ? 0.0 : 1.0;
+            double diff[4] = {0.0, 0.0, 0.0, 0.0};
+            if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
+            cell_update(m, s, P, g, me, F, diff, dt, pout, part);
         }
         tile_epilogue(m, s, tile, c, part, sh, false);
     }
@@ -591,38 +700,7 @@ __global__ void __launch_bounds__(256, MINB) k_face_update(const DevMesh m, cons
             }
             double diff[4] = {0.0, 0.0, 0.0, 0.0};
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
-            const double rarea = m.rarea[g];
-            const double4 U = s.U[g];
-            const double Uo[4] = {U.x, U.y, U.z, U.w};
-            double Un[4];
-            for (int v = 0; v < 4; ++v) Un[v] = (Uo[v] - F[v] * P.beta * dt * rarea + P.beta * dt * diff[v]);
-            if (P.density_constrained == 1) {
-                if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
-                if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
-            }
-            s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
-            const double gam = P.gamma;
-            const double rho = Un[0];
-            const double ux = Un[1] / Un[0];
-            const double uy = Un[2] / Un[0];
-            const double p = (gam - 1.0) * (Un[3] - 0.5 * (Un[1] * Un[1] + Un[2] * Un[2]) / Un[0]);
-            const double a = sqrt(gam * p / rho);
-            const double vmax = sqrt(ux * ux + uy * uy) + a;
-            pout[g] = make_double4(rho, ux, uy, p);
-            const double area = m.area[g];
-            for (int v = 0; v < 4; ++v) {
-                const double d = Un[v] - Uo[v];
-                part.res[v] = d * d;
-                part.tot[v] = Un[v] * area;
-            }
-            part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
-            part.vmax = vmax;
-            part.rmin = m.charlen[g] / vmax;
-            part.rhomin = me.x;
-            part.rhomax = me.x;
-            const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
-                            (p > 0.0);
-            part.bad = ok ? 0.0 : 1.0;
+            cell_update(m, s, P, g, me, F, diff, dt, pout, part);
         }
         tile_epilogue(m, s, tile, c, part, sh, false);
     }

@@ -1,8 +1,9 @@
 """Build recipe of the native library libgodunov2d.so (sm_100a).
 
-Two CUDA translation units get different floating-point contraction
-flags: kernels_f64.cu (the reference-exact FP64 path) is built with
--fmad=false; everything else with the default -fmad=true.  The library is
+The translation units get different floating-point flags: the
+reference-exact FP64 kernels (kernels_f64.cu, kernels_tf_f64.cu,
+gd2d_noalloc.cu) are built with -fmad=false, the mixed-precision kernels
+(kernels_mixed.cu, kernels_tf_mixed.cu) with -use_fast_math, the host code with the defaults.  The library is
 written in-tree next to this file so that it travels with the repository.
 """
 from __future__ import annotations
@@ -24,7 +25,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + CSRC, 
 # (source, extra flags)
 UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
+    ("kernels_tf_f64.cu", ["-fmad=false"]),
     ("kernels_mixed.cu", ["-use_fast_math"]),
+    ("kernels_tf_mixed.cu", ["-use_fast_math"]),
     ("gd2d_api.cu", []),
     ("gd2d_noalloc.cu", ["-fmad=false"]),
 ]

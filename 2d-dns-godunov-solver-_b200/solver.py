@@ -164,6 +164,18 @@ class Solver:
                                         Nd.ctypes.data_as(dp)))
         return {"Ucons": U, "prims": P, "node_prims": Nd}
 
+    def autotune(self, steps_per_trial: int = 64) -> dict:
+        """Time candidate launch shapes on this handle's own state (which is
+        saved and restored, so the run continues as if nothing happened) and
+        keep the fastest: cell-kernel register budget and persistence,
+        node-pass block, steps per CUDA graph.  Returns the chosen shape and
+        its device ms per step."""
+        ch = N.Launch()
+        self._chk(self.L.gd2d_autotune(self.h, int(steps_per_trial), C.byref(ch)))
+        t, _, _ = self.last_timing()
+        return {"min_blocks": ch.min_blocks, "persistent": ch.persistent, "node_block": ch.node_block,
+                "graph_steps": ch.graph_steps, "ms_per_step": t}
+
     def last_timing(self) -> Tuple[float, float, int]:
         t, c, n = C.c_double(), C.c_double(), C.c_int64()
         self._chk(self.L.gd2d_last_timing(self.h, C.byref(t), C.byref(c), C.byref(n)))

@@ -106,7 +106,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def build_workload(pkg, config: str, precision: str):
+def build_workload(pkg, config: str, precision: str, size: int = 1025):
     C = pkg.cases
     if config == "square":
         mesh, cfg, prims = C.square_inviscid(101)
@@ -121,11 +121,11 @@ def build_workload(pkg, config: str, precision: str):
         items = C.batched_cylinders(16)
         desc = {"workload": "batched_cylinders_16", "cases": 16, "cells": sum(m.nCells for m, _, _ in items)}
     else:
-        mesh, cfg, prims = C.cylinder_case(1025)
+        mesh, cfg, prims = C.cylinder_case(size)
         cfg = dict(cfg, dt_mode=2)
         items = [(mesh, cfg, prims)]
         desc = {"workload": "cylinder_viscous_fp64" if precision == "f64" else "cylinder_viscous_mixed",
-                "mesh": "[-5,15]x[-8,8] 1025^2 nodes, tris, r<0.5 removed", "cells": mesh.nCells,
+                "mesh": "[-5,15]x[-8,8] %d^2 nodes, tris, r<0.5 removed" % size, "cells": mesh.nCells,
                 "mach": 3.5, "re_d": 1.0e4, "limiter": "venkatakrishnan", "viscosity": "sutherland+artificial"}
     viscous = items[0][1].get("viscosity", "none") != "none"
     return items, desc, viscous
@@ -197,7 +197,7 @@ def mixed_variant(pkg, items, s64, args, peak):
     (bit-identical to the CPU oracle in the parity tests) from the same
     initial state."""
     mesh, cfg, prims = items[0]
-    sm = pkg.solver.Solver([mesh], [cfg], pkg.solver.make_launch(precision="mixed", order=args.order))
+    sm = pkg.solver.Solver([mesh], [cfg], pkg.solver.make_launch(precision="mixed", order=args.order, loop=args.loop))
     sm.createFields2d(0, *prims)
     sm.propagate2d(args.warmup)
     sm.propagate2d(args.steps)
@@ -238,6 +238,13 @@ def main():
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
     ap.add_argument("--order", default="hilbert")
     ap.add_argument("--graph-steps", type=int, default=0)
+    ap.add_argument("--loop", default="tile", choices=["cell", "tile"],
+                    help="cell-centred kernel or the tile-face kernel (same results)")
+    ap.add_argument("--min-blocks", type=int, default=0, help="cell-kernel register budget (0: library default)")
+    ap.add_argument("--node-block", type=int, default=0)
+    ap.add_argument("--size", type=int, default=1025, help="cylinder: nodes per side")
+    ap.add_argument("--autotune", action="store_true",
+                    help="let gd2d_autotune pick the launch shape before the warm-up")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     ap.add_argument("--error-steps", type=int, default=1000,
@@ -247,14 +254,14 @@ def main():
 
     world, rank, local, dist = dist_setup(args)
     pkg = graft.load_package()
-    items, desc, viscous = build_workload(pkg, args.config, args.precision)
+    items, desc, viscous = build_workload(pkg, args.config, args.precision, args.size)
     sharded = world > 1 and len(items) > 1
     if sharded:
         # independent cases split across ranks (no data exchange), balanced by cells
         mine = pkg.cases.shard_cases([m.nCells for m, _, _ in items], world, rank)
         items = [items[i] for i in mine]
     metric = "Mcell-steps/s"
-    cfg_line = dict(desc, precision=args.precision,
+    cfg_line = dict(desc, precision=args.precision, loop=args.loop,
                     parallelism=(("cases-sharded%d" if sharded else "replicas%d") % world), l2_flush="inputs > L2")
 
     if args.impl == "reference":
@@ -273,11 +280,14 @@ def main():
 
     meshes = [m for m, _, _ in items]
     cfgs = [c for _, c, _ in items]
-    launch = pkg.solver.make_launch(precision=args.precision, order=args.order, graph_steps=args.graph_steps)
+    launch = pkg.solver.make_launch(precision=args.precision, order=args.order, graph_steps=args.graph_steps,
+                                    loop=args.loop, min_blocks=args.min_blocks, node_block=args.node_block)
     s = pkg.solver.Solver(meshes, cfgs, launch)
     for i, (_, _, p) in enumerate(items):
         s.createFields2d(i, *p)
     cells = sum(m.nCells for m in meshes)
+    if args.autotune:
+        cfg_line["launch"] = s.autotune(64)
 
     # warm-up
     s.propagate2d(args.warmup)
@@ -325,7 +335,9 @@ def main():
             "data": "synthetic (seeded generated meshes and initial states)", "config": cfg_line,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": None,
-                         "kernel": "k_cell_step (fused reconstruction+flux+update)",
+                         "kernel": ("k_cell_step_tf" if args.loop == "tile" else "k_cell_step")
+                                   + (" (mixed)" if args.precision == "mixed" else "")
+                                   + " (fused reconstruction+flux+viscous+update)",
                          "alg_bytes_per_cell": alg, "cell_kernel_ms": cell_ms, "peak_kind": peak_kind,
                          "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak},
             "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},

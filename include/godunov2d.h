@@ -63,8 +63,13 @@ enum gd2d_order { GD2D_ORDER_NATURAL = 0, GD2D_ORDER_HILBERT = 1, GD2D_ORDER_RCM
  * twice, no atomics).  FACE_COLOURED: one thread per face, faces grouped in
  * colours no two of which touch the same cell, accumulating into the cells.
  * FACE_SLOTS: one thread per face, each side's flux stored in its own
- * (cell, face) slot and summed in face order by the update (FP64 only). */
-enum gd2d_loop { GD2D_LOOP_CELL = 0, GD2D_LOOP_FACE_COLOURED = 1, GD2D_LOOP_FACE_SLOTS = 2 };
+ * (cell, face) slot and summed in face order by the update (FP64 only).
+ * TILE_FACES: one fused kernel over per-tile face lists; a face between two
+ * cells of one tile is evaluated once when its flux is exactly antisymmetric
+ * (AUSM+ with Minmod/Venkatakrishnan/no limiter), results bit-identical to
+ * CELL (FP64 only). */
+enum gd2d_loop { GD2D_LOOP_CELL = 0, GD2D_LOOP_FACE_COLOURED = 1, GD2D_LOOP_FACE_SLOTS = 2,
+                 GD2D_LOOP_TILE_FACES = 3 };
 
 /* mesh2d_Int32 (primeObjects.jl:109-135) as read by readMesh2dHDF5
  * (utilsIO.jl:107-252).  All matrices column-major. */
@@ -196,9 +201,15 @@ int gd2d_cells_to_nodes(gd2d_handle *h);
 /* calcDiffTerm (calcDiffTerm.jl:31-121): Diff [nCells x 4] from Uold. */
 int gd2d_calc_diff_term(gd2d_handle *h, int32_t icase, double *diff);
 
-/* Autotuner: times candidate launch shapes on this handle's data and keeps
- * the fastest (block size, persistence, graph length).  The state is saved
- * and restored around the trials. */
+/* Autotuner (no counterpart in the reference, whose CPU loop has no launch
+ * shape): times candidate launch shapes on this handle's own data and keeps
+ * the fastest -- cell-kernel register budget (min_blocks 2/3/4) x
+ * persistence, node-pass block (64/128/256), steps per graph (8/32/128) --
+ * by coordinate search, `steps_per_trial` steps each (<= 0: 64).  Every
+ * device array a step touches is saved first and restored after the trials,
+ * so propagation continues bit-identically.  Needs gd2d_set_state on every
+ * case; allocates a temporary copy of the state.  `chosen` (may be NULL)
+ * receives the new launch shape; gd2d_last_timing's total is its ms/step. */
 int gd2d_autotune(gd2d_handle *h, int32_t steps_per_trial, gd2d_launch *chosen);
 
 /* Device time of the kernels of the last propagate call (CUDA events on the

@@ -43,12 +43,12 @@ def test_struct_layout_matches_header(pkg, tmp_path):
                      C.sizeof(N.BC), N.Params.bc.offset]
 
 
-def _setup(native, pkg, mesh, cfg, ncases=1):
+def _setup(native, pkg, mesh, cfg, ncases=1, launch=None):
     N = pkg._native
     views = (N.MeshView * ncases)(*[pkg.solver.mesh_view(mesh)] * ncases)
     params = (N.Params * ncases)(*[pkg.solver.make_params(cfg)] * ncases)
     h = C.c_void_p()
-    rc = native.gd2d_setup(C.byref(h), ncases, views, params, None)
+    rc = native.gd2d_setup(C.byref(h), ncases, views, params, C.byref(launch) if launch is not None else None)
     return rc, native.gd2d_last_error(None).decode()
 
 
@@ -76,7 +76,16 @@ def test_validation_errors_before_device_work(native, pkg):
     rc, msg = _setup(native, pkg, mesh, dict(cfg, CFL=-1.0))
     assert rc == -1
     assert native.gd2d_propagate(None, 1, None) == -1
+    assert native.gd2d_autotune(None, 8, None) == -1
     assert native.gd2d_destroy(None) == 0
+
+
+@pytest.mark.parametrize("shape,text", [({"block": 64}, "block"), ({"node_block": 512}, "node_block"),
+                                        ({"min_blocks": 5}, "min_blocks"), ({"precision": 7}, "precision")])
+def test_launch_shape_validation(native, pkg, shape, text):
+    mesh, cfg, _ = pkg.cases.square_inviscid(9)
+    rc, msg = _setup(native, pkg, mesh, cfg, launch=pkg.solver.make_launch(**shape))
+    assert rc == -1 and text in msg, (rc, msg)
 
 
 def test_missing_library_fails_loudly(pkg, tmp_path):

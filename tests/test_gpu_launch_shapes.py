@@ -1,0 +1,82 @@
+"""Launch shapes do not change results, and the autotuner leaves no trace.
+
+Every launch-shape knob of gd2d_launch (register budget, persistent grid,
+node-pass block, steps per graph, cell block) must give bit-identical FP64
+states: the per-tile reductions are ordered by tile, not by block, and each
+cell's arithmetic does not depend on where it runs.  gd2d_autotune runs
+trial steps on the handle's own state and must restore it exactly.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _viscous_case(pkg):
+    return pkg.cases.cylinder_case(129)
+
+
+def _run(pkg, mesh, cfg, prims, nsteps, **launch):
+    s = pkg.setupSolver(mesh, cfg, **launch)
+    s.createFields2d(0, *prims)
+    s.propagate2d(nsteps)
+    st = s.get_state(0)
+    h = s.history(0)
+    s.close()
+    return st, h
+
+
+@pytest.mark.parametrize("shape", [
+    {"min_blocks": 2}, {"min_blocks": 4}, {"persistent": 1}, {"persistent": 1, "min_blocks": 4},
+    {"node_block": 64}, {"node_block": 128}, {"block": 128}, {"graph_steps": 1}, {"graph_steps": 128},
+    {"loop": "tile"}, {"loop": "tile", "min_blocks": 2}, {"loop": "tile", "persistent": 1, "min_blocks": 4},
+])
+def test_launch_shape_is_bit_exact(pkg, shape):
+    mesh, cfg, prims = _viscous_case(pkg)
+    ref, href = _run(pkg, mesh, cfg, prims, 40)
+    got, hgot = _run(pkg, mesh, cfg, prims, 40, **shape)
+    for k in ("Ucons", "prims", "node_prims"):
+        assert np.array_equal(ref[k], got[k]), (shape, k)
+    assert [h["dt"] for h in href] == [h["dt"] for h in hgot]
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_autotune_restores_state(pkg, precision):
+    """The trials leave no trace: the state right after gd2d_autotune is the
+    state before it, and the run continues from there (FP64: bit-identical
+    to a run that never tuned; mixed: its FP32 arithmetic may round
+    differently under another register budget, so within 1e-6)."""
+    mesh, cfg, prims = _viscous_case(pkg)
+    ref, href = _run(pkg, mesh, cfg, prims, 30, precision=precision)
+    s = pkg.setupSolver(mesh, cfg, precision=precision)
+    s.createFields2d(0, *prims)
+    s.propagate2d(10)
+    before = s.get_state(0)
+    chosen = s.autotune(steps_per_trial=16)
+    after = s.get_state(0)
+    for k in ("Ucons", "prims", "node_prims"):
+        assert np.array_equal(before[k], after[k]), k
+    assert chosen["min_blocks"] in (2, 3, 4) and chosen["persistent"] in (0, 1)
+    assert chosen["node_block"] in (64, 128, 256) and chosen["graph_steps"] in (8, 32, 128)
+    assert chosen["ms_per_step"] > 0.0
+    s.propagate2d(20)
+    got = s.get_state(0)
+    h = s.history(0)
+    s.close()
+    assert len(h) == 30 and h[-1]["step"] == 30
+    if precision == "f64":
+        for k in ("Ucons", "prims", "node_prims"):
+            assert np.array_equal(ref[k], got[k]), k
+        assert [x["dt"] for x in h] == [x["dt"] for x in href]
+    else:
+        U, R = got["Ucons"], ref["Ucons"]
+        assert (np.abs(U - R).max(axis=0) / np.abs(R).max(axis=0)).max() <= 1e-6
+        assert h[-1]["flowTime"] == pytest.approx(href[-1]["flowTime"], rel=1e-6)
+
+
+def test_autotune_needs_state(pkg):
+    mesh, cfg, prims = _viscous_case(pkg)
+    s = pkg.setupSolver(mesh, cfg)
+    with pytest.raises(pkg._native.NativeError):
+        s.autotune(8)
+    s.close()

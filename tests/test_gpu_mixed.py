@@ -39,9 +39,10 @@ def run(pkg, orc, mesh, cfg, prims, nsteps, **launch):
     return s, o, s.history(0), oh
 
 
-def test_mixed_square_100_steps(pkg, orc):
+@pytest.mark.parametrize("loop", ["cell", "tile"])
+def test_mixed_square_100_steps(pkg, orc, loop):
     mesh, cfg, prims = pkg.cases.square_inviscid(101)
-    s, o, gh, oh = run(pkg, orc, mesh, cfg, prims, 100)
+    s, o, gh, oh = run(pkg, orc, mesh, cfg, prims, 100, loop=loop)
     U = s.get_state(0)["Ucons"]
     l2, linf = l2_linf(U, o.field("Uold"))
     print("mixed square 100 steps L2", l2, "Linf", linf)
@@ -52,9 +53,10 @@ def test_mixed_square_100_steps(pkg, orc):
     assert gh[-1]["dt"] == pytest.approx(oh[-1]["dt"], rel=1e-4)
 
 
-def test_mixed_cylinder_viscous(pkg, orc):
+@pytest.mark.parametrize("loop", ["cell", "tile"])
+def test_mixed_cylinder_viscous(pkg, orc, loop):
     mesh, cfg, prims = pkg.cases.cylinder_case(129)
-    s, o, gh, oh = run(pkg, orc, mesh, cfg, prims, 100)
+    s, o, gh, oh = run(pkg, orc, mesh, cfg, prims, 100, loop=loop)
     U = s.get_state(0)["Ucons"]
     l2, linf = l2_linf(U, o.field("Uold"))
     print("mixed cylinder 129 100 steps L2", l2, "Linf", linf)
@@ -62,10 +64,11 @@ def test_mixed_cylinder_viscous(pkg, orc):
     assert all(h["nonfinite"] == 0 for h in gh)
 
 
-@pytest.mark.parametrize("flux", ["roe", "ausm"])
-def test_mixed_fluxes_tgv_batch(pkg, orc, flux):
+@pytest.mark.parametrize("flux,loop", [("roe", "cell"), ("ausm", "cell"), ("roe", "tile"), ("ausm", "tile")])
+def test_mixed_fluxes_tgv_batch(pkg, orc, flux, loop):
     tg = [pkg.cases.tgv_case(n, 0.2 + 0.1 * k, 400.0 + 300 * k, flux=flux) for k, n in enumerate((33, 49, 41))]
-    s = pkg.solver.Solver([m for m, _, _ in tg], [c for _, c, _ in tg], pkg.solver.make_launch(precision="mixed"))
+    s = pkg.solver.Solver([m for m, _, _ in tg], [c for _, c, _ in tg],
+                          pkg.solver.make_launch(precision="mixed", loop=loop))
     for i, (_, _, p) in enumerate(tg):
         s.createFields2d(i, *p)
     s.propagate2d(50)
@@ -77,3 +80,10 @@ def test_mixed_fluxes_tgv_batch(pkg, orc, flux):
         assert l2[0] < 1e-5, (flux, i, l2)
         ek_gpu = s.history(i)[-1]["Ek"]
         assert ek_gpu == pytest.approx(oh[-1]["Ek"], rel=1e-5)
+
+
+def test_mixed_tile_quads(pkg, orc):
+    mesh, cfg, prims = pkg.cases.reference_tgv_case(41, quads=True)
+    s, o, gh, oh = run(pkg, orc, mesh, cfg, prims, 20, loop="tile")
+    l2, _ = l2_linf(s.get_state(0)["Ucons"], o.field("Uold"))
+    assert l2[0] < 1e-5 and l2.max() < 1e-4, l2

@@ -1,5 +1,7 @@
 """CPU checks of the mesh schema generators: the invariants the step
 relies on and the conventions of the reference's own mesh file."""
+import os
+
 import numpy as np
 import pytest
 
@@ -97,3 +99,42 @@ def test_hdf5_reader_matches_recorded_digests(pkg):
     assert len(ds) == 23
     for k, v in ds.items():
         assert hashlib.sha256(np.ascontiguousarray(np.asarray(v)).tobytes()).hexdigest() == meta["sha256"][k], k
+
+
+def _face_pair_symmetry(m):
+    """(interior faces, faces whose two slots are exact mirrors): normals
+    negated bit for bit, equal lengths, down/up nodes exchanged.  Those are
+    the faces the tile-face kernel may evaluate once for both cells."""
+    st, nx, ny, ln = m.cell_stiffness, m.cell_edges_Nx, m.cell_edges_Ny, m.cell_edges_length
+    dn, up, nf = m.node2cellL2down, m.node2cellL2up, m.mesh_connectivity[:, 2]
+    tot = good = 0
+    for a in range(m.nCells):
+        for k in range(nf[a]):
+            b = st[a, k] - 1
+            if b < 0:
+                continue
+            tot += 1
+            kb = [q for q in range(nf[b]) if st[b, q] - 1 == a]
+            if len(kb) != 1 or nf[a] != nf[b]:
+                continue
+            kb = kb[0]
+            ok = nx[b, kb] == -nx[a, k] and ny[b, kb] == -ny[a, k] and ln[b, kb] == ln[a, k]
+            ok = ok and dn[b, 2 * kb] == up[a, 2 * k] and up[b, 2 * kb] == dn[a, 2 * k]
+            if nf[a] == 4:
+                ok = ok and dn[b, 2 * kb + 1] == up[a, 2 * k + 1] and up[b, 2 * kb + 1] == dn[a, 2 * k + 1]
+            good += bool(ok)
+    return tot, good
+
+
+def test_generated_faces_are_exact_mirrors(pkg):
+    for m in (pkg.cases.square_inviscid(21)[0], pkg.cases.cylinder_case(41)[0],
+              pkg.cases.reference_tgv_case(13, quads=True)[0]):
+        tot, good = _face_pair_symmetry(m)
+        assert tot > 0 and good == tot
+
+
+def test_reference_mesh_face_mirrors(pkg):
+    m = pkg.mesh.Mesh2d.load_npz(os.path.join(os.path.dirname(__file__), "golden", "oblique_shock_mesh.npz"))
+    tot, good = _face_pair_symmetry(m)
+    print("reference mesh: %d of %d interior faces are exact mirrors" % (good, tot))
+    assert tot > 0
