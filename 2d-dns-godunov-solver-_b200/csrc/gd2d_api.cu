@@ -77,6 +77,7 @@ struct gd2d_handle {
     std::vector<std::vector<gd2d_stats>> history;
     std::vector<cudaEvent_t> ev;  // pairs around cell kernels of the captured graph
     cudaEvent_t ev_total[2] = {nullptr, nullptr};
+    cudaEvent_t ev_eager[2] = {nullptr, nullptr};  // around the cell kernel of the last eager step
     double last_total_ms = 0.0, last_cell_ms = 0.0;
     int64_t last_launches = 0;
     double4 *pinned = nullptr;  // page-locked staging for state uploads and downloads
@@ -352,8 +353,12 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         return fail(nullptr, GD2D_ERR_ARG, "node_block must be 64, 128 or 256");
     }
     h->lc.persistent = h->launch.persistent;
-    // FP64 cell kernel: 3 blocks/SM (128 registers); mixed: 4 (fewer live values)
-    h->lc.min_blocks = h->launch.min_blocks ? h->launch.min_blocks : (h->mixed ? 4 : 3);
+    // register budget of the cell kernel, measured best on the 2.09M-cell
+    // viscous cylinder: 3 blocks/SM for the FP64 cell-centred kernel, 4 for
+    // the FP64 tile-face kernel and for the mixed kernels
+    h->lc.min_blocks = h->launch.min_blocks
+                           ? h->launch.min_blocks
+                           : ((h->mixed || h->launch.loop == GD2D_LOOP_TILE_FACES) ? 4 : 3);
     if (h->lc.min_blocks < 2 || h->lc.min_blocks > 4) {
         delete h;
         return fail(nullptr, GD2D_ERR_ARG, "min_blocks must be 2, 3 or 4");
@@ -792,6 +797,8 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     h->cs_host.assign(n_cases, CaseState{});
     cudaEventCreate(&h->ev_total[0]);
     cudaEventCreate(&h->ev_total[1]);
+    cudaEventCreate(&h->ev_eager[0]);
+    cudaEventCreate(&h->ev_eager[1]);
     size_t maxn = 1;
     for (auto &c : h->cases) maxn = std::max<size_t>(maxn, std::max(c.nc, c.nn));
     {
@@ -906,14 +913,22 @@ static int64_t kernels_per_step(const gd2d_handle *h) {
 
 // The kernels of one step on the handle's stream: [viscous gradient passes]
 // -> fused cell kernel (bracketed by the optional timing events) -> node pass.
-static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, cudaEvent_t after_cell) {
+// Timing events inside a stream capture become external event-record nodes;
+// outside a capture they are plain records.
+static void record_timing(gd2d_handle *h, cudaEvent_t ev, bool in_capture) {
+    if (in_capture) cudaEventRecordWithFlags(ev, h->stream, cudaEventRecordExternal);
+    else cudaEventRecord(ev, h->stream);
+}
+
+static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, cudaEvent_t after_cell,
+                                       bool in_capture = false) {
     cudaError_t e = cudaSuccess;
     if (h->visc) {
         e = h->mixed ? launch_visc_grad_mixed(h->m, h->s, h->lc, h->stream)
                      : launch_visc_grad_f64(h->m, h->s, h->lc, h->stream);
         if (e != cudaSuccess) return e;
     }
-    if (before_cell) cudaEventRecordWithFlags(before_cell, h->stream, cudaEventRecordExternal);
+    if (before_cell) record_timing(h, before_cell, in_capture);
     if (h->loop == GD2D_LOOP_FACE_COLOURED) {
         for (size_t c = 0; c + 1 < h->colour_off.size(); ++c) {
             e = launch_face_flux_f64(h->m, h->s, h->flux, h->quads, false, h->d_faces, h->colour_off[c],
@@ -934,7 +949,7 @@ static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, 
                      : launch_cell_step_f64(h->m, h->s, h->flux, h->visc, h->quads, h->lc, h->stream);
     }
     if (e != cudaSuccess) return e;
-    if (after_cell) cudaEventRecordWithFlags(after_cell, h->stream, cudaEventRecordExternal);
+    if (after_cell) record_timing(h, after_cell, in_capture);
     return h->mixed ? launch_node_avg_mixed(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream)
                     : launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream);
 }
@@ -948,7 +963,7 @@ static int capture_graph(gd2d_handle *h, int steps, bool timing) {
     cudaGraph_t g;
     CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < steps; ++k) {
-        launch_step_kernels(h, timing ? h->ev[2 * k] : nullptr, timing ? h->ev[2 * k + 1] : nullptr);
+        launch_step_kernels(h, timing ? h->ev[2 * k] : nullptr, timing ? h->ev[2 * k + 1] : nullptr, true);
     }
     CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
@@ -989,8 +1004,10 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
                 launches += (int64_t)G * kernels_per_step(h);
             }
         }
+        const bool time_eager = !used_graph && k < chunk;
         for (; k < chunk; ++k) {
-            CUDA_TRY(h, launch_step_kernels(h, nullptr, nullptr));
+            const bool last = time_eager && k == chunk - 1;
+            CUDA_TRY(h, launch_step_kernels(h, last ? h->ev_eager[0] : nullptr, last ? h->ev_eager[1] : nullptr));
             launches += kernels_per_step(h);
         }
         CUDA_TRY(h, cudaEventRecord(h->ev_total[1], h->stream));
@@ -1007,6 +1024,13 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
                 }
             }
             (void)cudaGetLastError();  // a failed timing query must not surface at the next launch
+        } else if (time_eager) {
+            float c = 0.f;
+            if (cudaEventElapsedTime(&c, h->ev_eager[0], h->ev_eager[1]) == cudaSuccess) {
+                cell_ms += c;
+                ++cell_samples;
+            }
+            (void)cudaGetLastError();
         }
         // history
         // the chunk's ring rows (the ring is [ring_len][ncases]; rows wrap)
@@ -1372,6 +1396,7 @@ int gd2d_destroy(gd2d_handle *h) {
     cudaStreamSynchronize(h->stream);
     drop_graph(h);
     for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
+    for (auto &e : h->ev_eager) if (e) cudaEventDestroy(e);
     if (h->pinned) cudaFreeHost(h->pinned);
     h->buf.free_all();
     if (h->own_stream) cudaStreamDestroy(h->stream);

@@ -40,6 +40,13 @@ import __graft_entry__ as graft  # noqa: E402
 # cluster data; intermediates counted zero).
 ALG_BYTES = {("f64", False): 216, ("f64", True): 248, ("mixed", False): 164, ("mixed", True): 192}
 
+# DRAM bytes per cell of one cell-kernel launch on the viscous cylinder,
+# measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one
+# launch; FP64 cell-centred on 1025^2 nodes, the others on 513^2 nodes, the
+# traffic growing in proportion to the cells); None where not captured.
+CELL_KERNEL_TRAFFIC = {("f64", "cell"): 337.0, ("f64", "tile"): 368.0, ("mixed", "cell"): 233.0,
+                       ("mixed", "tile"): None}
+
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -329,12 +336,16 @@ def main():
     alg = ALG_BYTES[(args.precision, viscous)]
     achieved = alg * cells / (cell_ms / 1e3) / 1e9 if cell_ms > 0 else None
     step_achieved = alg * cells / (ms_per_step / 1e3) / 1e9
+    tpc = CELL_KERNEL_TRAFFIC.get((args.precision, args.loop)) if args.config == "cylinder" else None
+    traffic = tpc * cells if tpc else None
+    traffic_src = ("ncu dram bytes per cell of one launch x cells (%.0f B/cell)" % tpc) if tpc else None
     line = {"metric": metric, "value": value, "unit": "Mcell-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "f64" else "f32+f64",
             "data": "synthetic (seeded generated meshes and initial states)", "config": cfg_line,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "traffic_source": traffic_src,
                          "kernel": ("k_cell_step_tf" if args.loop == "tile" else "k_cell_step")
                                    + (" (mixed)" if args.precision == "mixed" else "")
                                    + " (fused reconstruction+flux+viscous+update)",
