@@ -77,8 +77,10 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
     }
 }
 
+// Node-side kernels: gather-latency bound, registers capped for 6
+// resident blocks per SM.
 template <bool VISC, bool UNIT>
-__global__ void __launch_bounds__(256) k_node_avg_mixed(const DevMesh m, const DevState s, int flip, int zero_prims,
+__global__ void __launch_bounds__(256, 6) k_node_avg_mixed(const DevMesh m, const DevState s, int flip, int zero_prims,
                                                         int64_t n0, int64_t n1) {
     const int par = *s.parity;
     const float4 *__restrict__ src = s.primf + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
@@ -137,7 +139,7 @@ __global__ void __launch_bounds__(256) k_node_avg_mixed(const DevMesh m, const D
 }
 
 template <bool QUAD>
-__global__ void __launch_bounds__(256) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
+__global__ void __launch_bounds__(256, 6) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         const int4 nb = m.nbr[g];
         if (nb.x == kAbsent) continue;
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(256) k_grad1_cells_mixed(const DevMesh m, cons
     }
 }
 
-__global__ void __launch_bounds__(256) k_grad1_nodes_mixed(const DevMesh m, const DevState s) {
+__global__ void __launch_bounds__(256, 6) k_grad1_nodes_mixed(const DevMesh m, const DevState s) {
     const int W = m.cluster_w;
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};

@@ -68,20 +68,21 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
             s_flux[tf.ka][tf.la] = make_float4(fv[0], fv[1], fv[2], fv[3]);
             if (tf.lbp) s_flux[tf.kb][tf.lbp - 1] = make_float4(-fv[0], -fv[1], -fv[2], -fv[3]);
         }
+        // the viscous source needs no flux: evaluated before the barrier
+        const int4 nb = m.nbr[g];
+        const bool is_quad = QUAD && (nb.w != kAbsent);
+        float diff[4] = {0.f, 0.f, 0.f, 0.f};
+        if (VISC && nb.x != kAbsent) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
         __syncthreads();
         Part part;
         part.init();
-        const int4 nb = m.nbr[g];
         if (nb.x != kAbsent) {
-            const bool is_quad = QUAD && (nb.w != kAbsent);
             const float4 a0 = s_flux[0][threadIdx.x], a1 = s_flux[1][threadIdx.x], a2 = s_flux[2][threadIdx.x];
             float F[4] = {a0.x + a1.x + a2.x, a0.y + a1.y + a2.y, a0.z + a1.z + a2.z, a0.w + a1.w + a2.w};
             if (QUAD && is_quad) {
                 const float4 a3 = s_flux[NS - 1][threadIdx.x];
                 F[0] += a3.x; F[1] += a3.y; F[2] += a3.z; F[3] += a3.w;
             }
-            float diff[4] = {0.f, 0.f, 0.f, 0.f};
-            if (VISC) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update_mixed(m, s, P, g, me, F, diff, dt, pout, part);
         }
         tile_epilogue(m, s, tile, c, part, sh, false);

@@ -431,12 +431,16 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
             s_flux[tf.ka][tf.la] = make_double4(fv[0], fv[1], fv[2], fv[3]);
             if (tf.lbp) s_flux[tf.kb][tf.lbp - 1] = make_double4(-fv[0], -fv[1], -fv[2], -fv[3]);
         }
+        // the cell's viscous source needs no flux: evaluated before the
+        // barrier, it fills the time a thread with fewer faces would wait
+        const int4 nb = m.nbr[g];
+        const bool is_quad = QUAD && (nb.w != kAbsent);
+        double diff[4] = {0.0, 0.0, 0.0, 0.0};
+        if (VISC && nb.x != kAbsent) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
         __syncthreads();
         Part part;
         part.init();
-        const int4 nb = m.nbr[g];
         if (nb.x != kAbsent) {
-            const bool is_quad = QUAD && (nb.w != kAbsent);
             const double4 a0 = s_flux[0][threadIdx.x], a1 = s_flux[1][threadIdx.x], a2 = s_flux[2][threadIdx.x];
             double F[4] = {a0.x + a1.x, a0.y + a1.y, a0.z + a1.z, a0.w + a1.w};
             F[0] = F[0] + a2.x; F[1] = F[1] + a2.y; F[2] = F[2] + a2.z; F[3] = F[3] + a2.w;
@@ -444,8 +448,6 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
                 const double4 a3 = s_flux[NS - 1][threadIdx.x];
                 F[0] = F[0] + a3.x; F[1] = F[1] + a3.y; F[2] = F[2] + a3.z; F[3] = F[3] + a3.w;
             }
-            double diff[4] = {0.0, 0.0, 0.0, 0.0};
-            if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update(m, s, P, g, me, F, diff, dt, pout, part);
         }
         tile_epilogue(m, s, tile, c, part, sh, false);
@@ -458,8 +460,11 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
 // weighted primitive averages; with VISC also calcPhiInCellCluster's
 // unweighted means of rho u, rho v, E (calcGradients.jl:3-18) for the next
 // step's viscous term.  The last block flips the step parity.
+// The node-side kernels are bound by the latency of their gathers; their
+// register budget is capped for 4 resident blocks per SM (more warps in
+// flight; measured faster than the unconstrained 76-register build).
 template <bool VISC, bool UNIT>
-__global__ void __launch_bounds__(256) k_node_avg(const DevMesh m, const DevState s, int flip, int zero_prims,
+__global__ void __launch_bounds__(256, 4) k_node_avg(const DevMesh m, const DevState s, int flip, int zero_prims,
                                                   int64_t n0, int64_t n1) {
     const int par = *s.parity;
     const double4 *__restrict__ src = s.prim + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
@@ -529,7 +534,7 @@ __global__ void __launch_bounds__(256) k_node_avg(const DevMesh m, const DevStat
 // means (calcScalarFieldGreenGaussNodesBasedGradient, calcGradients.jl:36-139:
 // gradX pairs with -ny, gradY with -nx).
 template <bool QUAD>
-__global__ void __launch_bounds__(256) k_grad1_cells(const DevMesh m, const DevState s) {
+__global__ void __launch_bounds__(256, 4) k_grad1_cells(const DevMesh m, const DevState s) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         const int4 nb = m.nbr[g];
         if (nb.x == kAbsent) continue;
@@ -559,7 +564,7 @@ __global__ void __launch_bounds__(256) k_grad1_cells(const DevMesh m, const DevS
 
 // Unweighted node means of the first gradients (calcPhiInCellCluster on the
 // gradient fields, calcGradients.jl:3-18).
-static __global__ void __launch_bounds__(256) k_grad1_nodes(const DevMesh m, const DevState s) {
+static __global__ void __launch_bounds__(256, 4) k_grad1_nodes(const DevMesh m, const DevState s) {
     const int W = m.cluster_w;
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
