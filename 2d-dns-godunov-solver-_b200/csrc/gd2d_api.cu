@@ -91,7 +91,8 @@ struct gd2d_handle {
     // single-function entry points
     double4 *split_unew = nullptr, *split_flux = nullptr, *split_delta = nullptr, *split_diff = nullptr;
     bool split_stage_done = false, split_diff_valid = false;
-    std::vector<CaseState> cs_host;
+    std::vector<CaseState> cs_host;  // host copy: steps taken per case (advanced by propagate)
+    DevStats *ring_host = nullptr;    // page-locked copy of the statistics ring
     std::string err;
 };
 
@@ -681,7 +682,17 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     double2 *d_mid = nullptr;
     int32_t *d_cl, *d_tc, *d_nc = nullptr;
     DevCase *d_cases;
-    auto bail = [&](int rc) { h->buf.free_all(); if (h->own_stream) cudaStreamDestroy(h->stream); g_setup_error = h->err; delete h; return rc; };
+    auto bail = [&](int rc) {
+        h->buf.free_all();
+        if (h->pinned) cudaFreeHost(h->pinned);
+        if (h->ring_host) cudaFreeHost(h->ring_host);
+        for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
+        for (auto &e : h->ev_eager) if (e) cudaEventDestroy(e);
+        if (h->own_stream) cudaStreamDestroy(h->stream);
+        g_setup_error = h->err;
+        delete h;
+        return rc;
+    };
 #define ALLOC(ptr, n)                                                                              \
     do {                                                                                           \
         cudaError_t e__ = h->buf.alloc(&(ptr), (size_t)(n));                                       \
@@ -805,6 +816,8 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         cudaError_t e = cudaMallocHost((void **)&h->pinned, maxn * sizeof(double4));
         if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaMallocHost: %s", cudaGetErrorString(e)));
         h->pinned_count = maxn;
+        e = cudaMallocHost((void **)&h->ring_host, sizeof(DevStats) * (size_t)s.ring_len * n_cases);
+        if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaMallocHost: %s", cudaGetErrorString(e)));
     }
     // uploads above went through the legacy stream; finish them before any
     // work is queued on the handle's stream
@@ -983,12 +996,17 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
     double total_ms = 0.0, cell_ms = 0.0;
     int cell_samples = 0;
     int32_t done = 0;
-    std::vector<int64_t> step0(h->ncases);
+    const int64_t RL = h->s.ring_len;
     while (done < nsteps) {
         const int32_t chunk = std::min<int32_t>(nsteps - done, h->s.ring_len);
-        std::vector<CaseState> before(h->ncases);
-        int rc0 = copy_sync(h, before.data(), h->s.cstate, sizeof(CaseState) * h->ncases, cudaMemcpyDeviceToHost);
-        if (rc0) return rc0;
+        // steps taken so far per case, kept on the host (the device's copy
+        // advances in step with it): no read-back before the launches
+        std::vector<int64_t> step0(h->ncases);
+        bool lockstep = true;
+        for (int c = 0; c < h->ncases; ++c) {
+            step0[c] = h->cs_host[c].step;
+            lockstep &= step0[c] == step0[0];
+        }
         CUDA_TRY(h, cudaEventRecord(h->ev_total[0], h->stream));
         int32_t k = 0;
         bool used_graph = false;
@@ -1011,6 +1029,21 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
             launches += kernels_per_step(h);
         }
         CUDA_TRY(h, cudaEventRecord(h->ev_total[1], h->stream));
+        // the chunk's statistics rows (the ring is [ring_len][ncases], rows
+        // wrap; cases whose step counts differ -- one re-initialised in mid
+        // run -- sit in different rows, then the whole ring is read)
+        if (lockstep) {
+            const int64_t r0 = step0[0] % RL;
+            const int64_t first = std::min<int64_t>(chunk, RL - r0);
+            CUDA_TRY(h, cudaMemcpyAsync(h->ring_host + r0 * h->ncases, h->s.ring + r0 * h->ncases,
+                                        sizeof(DevStats) * first * h->ncases, cudaMemcpyDeviceToHost, h->stream));
+            if (first < chunk)
+                CUDA_TRY(h, cudaMemcpyAsync(h->ring_host, h->s.ring, sizeof(DevStats) * (chunk - first) * h->ncases,
+                                            cudaMemcpyDeviceToHost, h->stream));
+        } else {
+            CUDA_TRY(h, cudaMemcpyAsync(h->ring_host, h->s.ring, sizeof(DevStats) * RL * h->ncases,
+                                        cudaMemcpyDeviceToHost, h->stream));
+        }
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         float ms = 0.f;
         cudaEventElapsedTime(&ms, h->ev_total[0], h->ev_total[1]);
@@ -1032,24 +1065,11 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
             }
             (void)cudaGetLastError();
         }
-        // history
-        // the chunk's ring rows (the ring is [ring_len][ncases]; rows wrap)
-        std::vector<DevStats> ring((size_t)h->s.ring_len * h->ncases);
-        {
-            const int64_t r0 = before[0].step % h->s.ring_len;
-            const int64_t first = std::min<int64_t>(chunk, h->s.ring_len - r0);
-            CUDA_TRY(h, cudaMemcpyAsync(ring.data() + r0 * h->ncases, h->s.ring + r0 * h->ncases,
-                                        sizeof(DevStats) * first * h->ncases, cudaMemcpyDeviceToHost, h->stream));
-            if (first < chunk)
-                CUDA_TRY(h, cudaMemcpyAsync(ring.data(), h->s.ring, sizeof(DevStats) * (chunk - first) * h->ncases,
-                                            cudaMemcpyDeviceToHost, h->stream));
-            CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-        }
         bool bad = false;
         for (int c = 0; c < h->ncases; ++c) {
             for (int32_t q = 0; q < chunk; ++q) {
-                int64_t stp = before[c].step + q;
-                const DevStats &ds = ring[(size_t)(stp % h->s.ring_len) * h->ncases + c];
+                int64_t stp = step0[c] + q;
+                const DevStats &ds = h->ring_host[(size_t)(stp % RL) * h->ncases + c];
                 gd2d_stats st;
                 static_assert(sizeof(gd2d_stats) == sizeof(DevStats), "stats layout");
                 std::memcpy(&st, &ds, sizeof st);
@@ -1057,10 +1077,11 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
                 bad |= st.nonfinite != 0;
             }
             if (stats_out) stats_out[c] = h->history[c].back();
+            h->cs_host[c].step = step0[c] + chunk;
         }
         done += chunk;
         if (bad) return fail(h, GD2D_ERR_NONFINITE, "non-finite or non-positive state after step %lld",
-                             (long long)(before[0].step + chunk));
+                             (long long)(step0[0] + chunk));
     }
     h->last_total_ms = total_ms;
     h->last_cell_ms = cell_samples ? cell_ms / cell_samples : 0.0;
@@ -1398,6 +1419,7 @@ int gd2d_destroy(gd2d_handle *h) {
     for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
     for (auto &e : h->ev_eager) if (e) cudaEventDestroy(e);
     if (h->pinned) cudaFreeHost(h->pinned);
+    if (h->ring_host) cudaFreeHost(h->ring_host);
     h->buf.free_all();
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;

@@ -182,6 +182,33 @@ def test_batched_cases_match_individual_oracles(pkg, orc):
         assert relerr(s2.get_state(i)["Ucons"], o.field("Uold")) <= TOL_100, i
 
 
+def test_reinitialised_case_in_a_batch(pkg):
+    """One case of a batched handle re-initialised in mid run: the other
+    case's history continues, the re-initialised case starts again at step
+    1 with statistics equal to a fresh handle's (cases never interact)."""
+    items = [pkg.cases.square_inviscid(21, seed=2), pkg.cases.square_inviscid(37, seed=3)]
+    s = pkg.solver.Solver([m for m, _, _ in items], [c for _, c, _ in items], pkg.solver.make_launch())
+    for i, (_, _, p) in enumerate(items):
+        s.createFields2d(i, *p)
+    s.propagate2d(5)
+    s.createFields2d(1, *items[1][2])
+    s.propagate2d(3)
+    h0, h1 = s.history(0), s.history(1)
+    assert [h["step"] for h in h0] == list(range(1, 9))
+    assert [h["step"] for h in h1] == [1, 2, 3]
+    U1 = s.get_state(1)["Ucons"]
+    s.close()
+    m, c, p = items[1]
+    f = pkg.solver.Solver([m], [c], pkg.solver.make_launch())
+    f.createFields2d(0, *p)
+    f.propagate2d(3)
+    hf = f.history(0)
+    assert np.array_equal(U1, f.get_state(0)["Ucons"])
+    assert [h["dt"] for h in hf] == [h["dt"] for h in h1]
+    assert [h["residual"] for h in hf] == [h["residual"] for h in h1]
+    f.close()
+
+
 def test_nonfinite_state_is_reported(pkg):
     mesh, cfg, prims = pkg.cases.square_inviscid(21)
     rho, u, v, p = [np.array(x, dtype=np.float64) for x in prims]
