@@ -86,6 +86,7 @@ struct gd2d_handle {
     int loop = GD2D_LOOP_CELL;
     int4 *d_faces = nullptr;
     int64_t nfaces = 0;
+    int64_t ngroups = 0;  // tile groups of the step reduction, all cases
     std::vector<int64_t> colour_off;
     double4 *Facc = nullptr, *Fslot = nullptr;
     // single-function entry points
@@ -479,6 +480,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     std::vector<int32_t> tile_case(ntiles, 0);
     std::vector<int32_t> node_case(Nn, 0);
     h->hcases.resize(n_cases);
+    int64_t ngroups = 0;
     for (int c = 0; c < n_cases; ++c) {
         const gd2d_mesh_view &mv = meshes[c];
         HostCase &hc = h->cases[c];
@@ -548,12 +550,16 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         d.cell_end = hc.cell_off + hc.nc_pad;
         d.tile_begin = hc.cell_off / block;
         d.tile_end = (hc.cell_off + hc.nc_pad) / block;
+        d.group_begin = ngroups;
+        ngroups += (d.tile_end - d.tile_begin + kGroupTiles - 1) / kGroupTiles;
+        d.group_end = ngroups;
         for (int64_t t = d.tile_begin; t < d.tile_end; ++t) tile_case[t] = c;
         const int64_t node_end = (c + 1 < n_cases) ? h->cases[c + 1].node_off : Nn;
         for (int64_t j = hc.node_off; j < node_end; ++j) node_case[j] = c;
         h->hcases[c] = d;
     }
     h->tile_case_h = tile_case;
+    h->ngroups = ngroups;
 
     // face list for the face-loop variants: each interior face once (from its
     // lower-indexed cell), boundary faces once; greedy edge colouring so that
@@ -797,6 +803,8 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     ALLOC(s.ring, (size_t)s.ring_len * n_cases);
     ALLOC(s.parity, 1);
     ALLOC(s.node_done, 1);
+    ALLOC(s.gpart, (size_t)ngroups * kPartials);
+    ALLOC(s.group_done, ngroups);
 #undef ALLOC
 #undef UPLOAD
     {
@@ -1274,6 +1282,8 @@ std::vector<Region> step_state(const gd2d_handle *h) {
     add(s.ring, sizeof(DevStats) * s.ring_len * m.ncases);
     add(s.parity, sizeof(int32_t));
     add(s.node_done, sizeof(unsigned int));
+    add(s.gpart, sizeof(double) * h->ngroups * kPartials);
+    add(s.group_done, sizeof(unsigned int) * h->ngroups);
     add(h->Facc, sizeof(double4) * m.Nc);
     add(h->Fslot, sizeof(double4) * m.nfmax * m.Nc);
     return r;

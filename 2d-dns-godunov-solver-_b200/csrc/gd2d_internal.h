@@ -25,6 +25,7 @@ constexpr int kCellPad = 1024;      // case cell ranges are multiples of this
 constexpr int kMaxBC = 8;
 constexpr int32_t kAbsent = INT32_MIN;
 constexpr int kPartials = 16;       // doubles per tile partial record
+constexpr int kGroupTiles = 256;    // tiles per group of the two-level step reduction
 constexpr int kMaxCluster = 8;
 
 enum FluxKind { FLUX_AUSM = 1, FLUX_ROE = 2, FLUX_AUSM_M2020 = 3 };
@@ -51,13 +52,14 @@ struct DevCase {
     int32_t density_constrained, pad_;
     int64_t cell_begin, cell_end;   // padded global cell range [begin, end)
     int64_t tile_begin, tile_end;   // tiles of the cell kernel
+    int64_t group_begin, group_end; // tile groups (kGroupTiles tiles each, the last one shorter)
 };
 
 // Per-case mutable step state (device).
 struct CaseState {
     double t, dt, velmax, rmin;
     int64_t step;
-    unsigned int tiles_done;
+    unsigned int tiles_done;  // tile groups of the case finished this step
     int32_t nonfinite;
 };
 
@@ -140,6 +142,8 @@ struct DevState {
     NodeGrad *g1;      // [Nc] (viscous) first gradients per cell
     NodeGrad *nodeG;   // [Nn] (viscous)
     double *part;      // [ntiles][kPartials]
+    double *gpart;     // [ngroups][kPartials] group records
+    unsigned int *group_done;  // [ngroups] tiles of the group finished this step
     CaseState *cstate; // [ncases]
     DevStats *ring;    // [ring_len][ncases]
     int32_t *parity;   // step parity (which prim buffer is current)

@@ -78,17 +78,17 @@ __device__ __forceinline__ void block_reduce(Part &p, Part *sh) {
     __syncthreads();
 }
 
-// Per-case finalization by the block that completed the case's last tile:
-// reduce the tile records in a fixed order, publish the step statistics and
-// advance time (flowTime += dt, testInviscidFluxesGPUx32.jl:401) and the
-// next dt (tau at :322-324, or the local-CFL extension).
+// Per-case finalization by the block that completed the case's last tile
+// group: reduce the group records in a fixed order, publish the step
+// statistics and advance time (flowTime += dt, testInviscidFluxesGPUx32.jl:401)
+// and the next dt (tau at :322-324, or the local-CFL extension).
 static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c, Part *sh, bool is_init) {
     const DevCase &P = m.cases[c];
     Part acc;
     acc.init();
-    for (int64_t t = P.tile_begin + threadIdx.x; t < P.tile_end; t += blockDim.x) {
+    for (int64_t q = P.group_begin + threadIdx.x; q < P.group_end; q += blockDim.x) {
         Part o;
-        o.load_cg(s.part + t * kPartials);
+        o.load_cg(s.gpart + q * kPartials);
         acc.combine(o);
     }
     block_reduce(acc, sh);
@@ -124,23 +124,51 @@ static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c,
     }
 }
 
-// Publish the tile record and, if this tile completes its case, finalize it.
+// Publish the tile record; the block that completes a group of kGroupTiles
+// tiles reduces the group (fixed order) into a group record, and the block
+// that completes a case's last group finalizes the case.  Two short levels
+// instead of one long one: the serial tail at the end of the kernel reads
+// at most one record per thread per level.  Whichever block ends up doing
+// a reduction, its order is the same, so the results are deterministic.
 __device__ __forceinline__ void tile_epilogue(const DevMesh &m, const DevState &s, int64_t tile, int c, Part &p,
                                               Part *sh, bool is_init) {
-    __shared__ int s_last;
+    __shared__ int s_last_group, s_last_case;
+    const DevCase &P = m.cases[c];
+    const int64_t gi = (tile - P.tile_begin) / kGroupTiles;
+    const int64_t gid = P.group_begin + gi;
+    const int64_t t0 = P.tile_begin + gi * kGroupTiles;
+    const int64_t t1 = (t0 + kGroupTiles < P.tile_end) ? t0 + kGroupTiles : P.tile_end;
     block_reduce(p, sh);
     if (threadIdx.x == 0) {
         p.store(s.part + tile * kPartials);
         __threadfence();
-        const DevCase &P = m.cases[c];
-        unsigned int ntile = (unsigned int)(P.tile_end - P.tile_begin);
-        unsigned int prev = atomicAdd(&s.cstate[c].tiles_done, 1u);
-        s_last = (prev == ntile - 1u) ? 1 : 0;
+        const unsigned int prev = atomicAdd(&s.group_done[gid], 1u);
+        s_last_group = (prev == (unsigned int)(t1 - t0) - 1u) ? 1 : 0;
     }
     __syncthreads();
-    if (s_last) {
+    if (s_last_group) {
         __threadfence();
-        finalize_case(m, s, c, sh, is_init);
+        Part acc;
+        acc.init();
+        for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+            Part o;
+            o.load_cg(s.part + t * kPartials);
+            acc.combine(o);
+        }
+        block_reduce(acc, sh);
+        if (threadIdx.x == 0) {
+            acc.store(s.gpart + gid * kPartials);
+            s.group_done[gid] = 0u;
+            __threadfence();
+            const unsigned int ng = (unsigned int)(P.group_end - P.group_begin);
+            const unsigned int prev = atomicAdd(&s.cstate[c].tiles_done, 1u);
+            s_last_case = (prev == ng - 1u) ? 1 : 0;
+        }
+        __syncthreads();
+        if (s_last_case) {
+            __threadfence();
+            finalize_case(m, s, c, sh, is_init);
+        }
     }
     __syncthreads();
 }
