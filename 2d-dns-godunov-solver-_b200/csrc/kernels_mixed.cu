@@ -97,23 +97,28 @@ __global__ void __launch_bounds__(256, 6) k_node_avg_mixed(const DevMesh m, cons
         float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f, det = 0.f;
         float c0 = 0.f, c1 = 0.f, c2 = 0.f;
         int cnt = 0;
-        for (int j = 0; j < W; ++j) {
-            const int c = m.cl[(int64_t)j * m.Nn + J];
-            if (c >= 0) {
-                const float w = UNIT ? 1.f : (float)m.wt[(int64_t)j * m.Nn + J];
-                const float4 p = src[c];
-                a0 += p.x * w; a1 += p.y * w; a2 += p.z * w; a3 += p.w * w;
-                det += w;
-                if (VISC) {
-                    if (prim_form) {
-                        c0 += p.y; c1 += p.z; c2 += 0.5f * (p.y * p.y + p.z * p.z) + gop * (p.w / ((gam - 1.f) * p.x));
-                    } else {
-                        const double4 u = s.U[c];
-                        c0 += (float)u.y; c1 += (float)u.z; c2 += (float)u.w;
-                    }
-                    ++cnt;
+        auto add = [&](int c, const float4 &p, float w) {
+            a0 += p.x * w; a1 += p.y * w; a2 += p.z * w; a3 += p.w * w;
+            det += w;
+            if (VISC) {
+                if (prim_form) {
+                    c0 += p.y; c1 += p.z; c2 += 0.5f * (p.y * p.y + p.z * p.z) + gop * (p.w / ((gam - 1.f) * p.x));
+                } else {
+                    const double4 u = s.U[c];
+                    c0 += (float)u.y; c1 += (float)u.z; c2 += (float)u.w;
                 }
+                ++cnt;
             }
+        };
+        int ci[kMaxCluster];
+#pragma unroll
+        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? m.cl[(int64_t)j * m.Nn + J] : -1;
+#pragma unroll
+        for (int j = 0; j < kMaxCluster; ++j)
+            if (ci[j] >= 0) add(ci[j], src[ci[j]], UNIT ? 1.f : (float)m.wt[(int64_t)j * m.Nn + J]);
+        for (int j = kMaxCluster; j < W; ++j) {
+            const int c = m.cl[(int64_t)j * m.Nn + J];
+            if (c >= 0) add(c, src[c], UNIT ? 1.f : (float)m.wt[(int64_t)j * m.Nn + J]);
         }
         if (det != 0.f) { const float r = 1.f / det; a0 *= r; a1 *= r; a2 *= r; a3 *= r; }
         s.nodePf[J] = zero_prims ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(a0, a1, a2, a3);
@@ -168,13 +173,19 @@ __global__ void __launch_bounds__(256, 6) k_grad1_nodes_mixed(const DevMesh m, c
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int cnt = 0;
-        for (int j = 0; j < W; ++j) {
+        auto add = [&](const NodeGradF &q) {
+            v[0] += q.ru.x; v[1] += q.ru.y; v[2] += q.rv.x; v[3] += q.rv.y; v[4] += q.re.x; v[5] += q.re.y;
+            ++cnt;
+        };
+        int ci[kMaxCluster];
+#pragma unroll
+        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? m.cl[(int64_t)j * m.Nn + J] : -1;
+#pragma unroll
+        for (int j = 0; j < kMaxCluster; ++j)
+            if (ci[j] >= 0) add(s.g1f[ci[j]]);
+        for (int j = kMaxCluster; j < W; ++j) {
             const int c = m.cl[(int64_t)j * m.Nn + J];
-            if (c >= 0) {
-                const NodeGradF q = s.g1f[c];
-                v[0] += q.ru.x; v[1] += q.ru.y; v[2] += q.rv.x; v[3] += q.rv.y; v[4] += q.re.x; v[5] += q.re.y;
-                ++cnt;
-            }
+            if (c >= 0) add(s.g1f[c]);
         }
         const float r = cnt ? 1.f / (float)cnt : 0.f;
         NodeGradF o;

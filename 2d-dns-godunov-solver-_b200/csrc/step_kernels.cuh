@@ -509,25 +509,32 @@ __global__ void __launch_bounds__(256, 4) k_node_avg(const DevMesh m, const DevS
         double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, det = 0.0;
         double c0 = 0.0, c1 = 0.0, c2 = 0.0;
         int cnt = 0;
-        for (int j = 0; j < W; ++j) {
-            const int c = m.cl[(int64_t)j * m.Nn + J];
-            if (c >= 0) {
-                const double w = UNIT ? 1.0 : m.wt[(int64_t)j * m.Nn + J];
-                const double4 p = src[c];
-                a0 = a0 + p.x * w; a1 = a1 + p.y * w; a2 = a2 + p.z * w; a3 = a3 + p.w * w;
-                det = det + w;
-                if (VISC) {
-                    if (prim_form) {
-                        // u, v, phi = |u|^2/2 + (gamma/Pr) p / ((gamma-1) rho)
-                        const double ph = 0.5 * (p.y * p.y + p.z * p.z) + gop * (p.w / ((gam - 1.0) * p.x));
-                        c0 = c0 + p.y; c1 = c1 + p.z; c2 = c2 + ph;
-                    } else {
-                        const double4 u = s.U[c];
-                        c0 = c0 + u.y; c1 = c1 + u.z; c2 = c2 + u.w;
-                    }
-                    ++cnt;
+        auto add = [&](int c, const double4 &p, double w) {
+            a0 = a0 + p.x * w; a1 = a1 + p.y * w; a2 = a2 + p.z * w; a3 = a3 + p.w * w;
+            det = det + w;
+            if (VISC) {
+                if (prim_form) {
+                    // u, v, phi = |u|^2/2 + (gamma/Pr) p / ((gamma-1) rho)
+                    const double ph = 0.5 * (p.y * p.y + p.z * p.z) + gop * (p.w / ((gam - 1.0) * p.x));
+                    c0 = c0 + p.y; c1 = c1 + p.z; c2 = c2 + ph;
+                } else {
+                    const double4 u = s.U[c];
+                    c0 = c0 + u.y; c1 = c1 + u.z; c2 = c2 + u.w;
                 }
+                ++cnt;
             }
+        };
+        // all cluster indices first, then the gathers in an unrolled
+        // sequence the compiler can overlap (sums keep the reference order)
+        int ci[kMaxCluster];
+#pragma unroll
+        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? m.cl[(int64_t)j * m.Nn + J] : -1;
+#pragma unroll
+        for (int j = 0; j < kMaxCluster; ++j)
+            if (ci[j] >= 0) add(ci[j], src[ci[j]], UNIT ? 1.0 : m.wt[(int64_t)j * m.Nn + J]);
+        for (int j = kMaxCluster; j < W; ++j) {
+            const int c = m.cl[(int64_t)j * m.Nn + J];
+            if (c >= 0) add(c, src[c], UNIT ? 1.0 : m.wt[(int64_t)j * m.Nn + J]);
         }
         if (det != 0.0) { a0 = a0 / det; a1 = a1 / det; a2 = a2 / det; a3 = a3 / det; }
         s.nodeP[J] = zero_prims ? make_double4(0.0, 0.0, 0.0, 0.0) : make_double4(a0, a1, a2, a3);
@@ -597,14 +604,20 @@ static __global__ void __launch_bounds__(256, 4) k_grad1_nodes(const DevMesh m, 
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         int cnt = 0;
-        for (int j = 0; j < W; ++j) {
+        auto add = [&](const NodeGrad &q) {
+            v[0] = v[0] + q.ru.x; v[1] = v[1] + q.ru.y; v[2] = v[2] + q.rv.x;
+            v[3] = v[3] + q.rv.y; v[4] = v[4] + q.re.x; v[5] = v[5] + q.re.y;
+            ++cnt;
+        };
+        int ci[kMaxCluster];
+#pragma unroll
+        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? m.cl[(int64_t)j * m.Nn + J] : -1;
+#pragma unroll
+        for (int j = 0; j < kMaxCluster; ++j)
+            if (ci[j] >= 0) add(s.g1[ci[j]]);
+        for (int j = kMaxCluster; j < W; ++j) {
             const int c = m.cl[(int64_t)j * m.Nn + J];
-            if (c >= 0) {
-                const NodeGrad q = s.g1[c];
-                v[0] = v[0] + q.ru.x; v[1] = v[1] + q.ru.y; v[2] = v[2] + q.rv.x;
-                v[3] = v[3] + q.rv.y; v[4] = v[4] + q.re.x; v[5] = v[5] + q.re.y;
-                ++cnt;
-            }
+            if (c >= 0) add(s.g1[c]);
         }
         NodeGrad r;
         if (cnt != 0) {
