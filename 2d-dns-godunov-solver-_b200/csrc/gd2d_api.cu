@@ -28,6 +28,7 @@ thread_local std::string g_setup_error;
 struct HostCase {
     int64_t nc = 0, nn = 0, nc_pad = 0;
     int64_t cell_off = 0, node_off = 0;
+    int64_t ref_off = 0, nref_off = 0;        // offsets in the compact reference-order index arrays
     std::vector<int64_t> cell_perm, cell_inv;  // perm[new] = old, inv[old] = new
     std::vector<int64_t> node_perm, node_inv;
     gd2d_params params{};
@@ -80,8 +81,11 @@ struct gd2d_handle {
     cudaEvent_t ev_eager[2] = {nullptr, nullptr};  // around the cell kernel of the last eager step
     double last_total_ms = 0.0, last_cell_ms = 0.0;
     int64_t last_launches = 0;
-    double4 *pinned = nullptr;  // page-locked staging for state uploads and downloads
-    size_t pinned_count = 0;
+    // reordering between reference and device order, on the device
+    int32_t *d_perm = nullptr;   // [Nc] reference row of each device cell
+    int32_t *d_inv = nullptr;    // [sum nc] device cell of each reference row
+    int32_t *d_ninv = nullptr;   // [sum nn] device node of each reference node
+    double *d_stage = nullptr;   // [4 x max(nc, nn)] reference-order columns in transit
     // face-loop variants: faces sorted by colour, colour ranges, flux storage
     int loop = GD2D_LOOP_CELL;
     int4 *d_faces = nullptr;
@@ -391,7 +395,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
 
     // ------------------------------------------------------- ordering
     h->cases.resize(n_cases);
-    int64_t Nc = 0, Nn = 0;
+    int64_t Nc = 0, Nn = 0, NcRef = 0, NnRef = 0;
     int W = 1;
     bool unit = true;
     for (int c = 0; c < n_cases; ++c) {
@@ -404,6 +408,10 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         hc.nc_pad = (hc.nc + kCellPad - 1) / kCellPad * kCellPad;
         hc.cell_off = Nc;
         hc.node_off = Nn;
+        hc.ref_off = NcRef;
+        hc.nref_off = NnRef;
+        NcRef += hc.nc;
+        NnRef += hc.nn;
         Nc += hc.nc_pad;
         Nn += (hc.nn + 3) / 4 * 4;
         for (int b = 0; b < params[c].n_bc; ++b) h->tgv |= params[c].bc[b].kind == GD2D_BC_TGV_ANALYTIC;
@@ -690,7 +698,6 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     DevCase *d_cases;
     auto bail = [&](int rc) {
         h->buf.free_all();
-        if (h->pinned) cudaFreeHost(h->pinned);
         if (h->ring_host) cudaFreeHost(h->ring_host);
         for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
         for (auto &e : h->ev_eager) if (e) cudaEventDestroy(e);
@@ -805,6 +812,20 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     ALLOC(s.node_done, 1);
     ALLOC(s.gpart, (size_t)ngroups * kPartials);
     ALLOC(s.group_done, ngroups);
+    {
+        std::vector<int32_t> perm(Nc, 0), inv(NcRef, 0), ninv(NnRef, 0);
+        int64_t maxrows = 1;
+        for (const HostCase &hc : h->cases) {
+            for (int64_t j = 0; j < hc.nc; ++j) perm[hc.cell_off + j] = (int32_t)hc.cell_perm[j];
+            for (int64_t i = 0; i < hc.nc; ++i) inv[hc.ref_off + i] = (int32_t)hc.cell_inv[i];
+            for (int64_t i = 0; i < hc.nn; ++i) ninv[hc.nref_off + i] = (int32_t)hc.node_inv[i];
+            maxrows = std::max(maxrows, std::max(hc.nc, hc.nn));
+        }
+        ALLOC(h->d_perm, perm.size()); UPLOAD(h->d_perm, perm);
+        ALLOC(h->d_inv, inv.size()); UPLOAD(h->d_inv, inv);
+        ALLOC(h->d_ninv, ninv.size()); UPLOAD(h->d_ninv, ninv);
+        ALLOC(h->d_stage, (size_t)4 * maxrows);
+    }
 #undef ALLOC
 #undef UPLOAD
     {
@@ -818,13 +839,8 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     cudaEventCreate(&h->ev_total[1]);
     cudaEventCreate(&h->ev_eager[0]);
     cudaEventCreate(&h->ev_eager[1]);
-    size_t maxn = 1;
-    for (auto &c : h->cases) maxn = std::max<size_t>(maxn, std::max(c.nc, c.nn));
     {
-        cudaError_t e = cudaMallocHost((void **)&h->pinned, maxn * sizeof(double4));
-        if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaMallocHost: %s", cudaGetErrorString(e)));
-        h->pinned_count = maxn;
-        e = cudaMallocHost((void **)&h->ring_host, sizeof(DevStats) * (size_t)s.ring_len * n_cases);
+        cudaError_t e = cudaMallocHost((void **)&h->ring_host, sizeof(DevStats) * (size_t)s.ring_len * n_cases);
         if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaMallocHost: %s", cudaGetErrorString(e)));
     }
     // uploads above went through the legacy stream; finish them before any
@@ -858,18 +874,22 @@ static int drop_graph(gd2d_handle *h) {
     return GD2D_OK;
 }
 
-// The cell primitives of one case, already permuted into the pinned staging
-// buffer, become the case's state: U, the node fields and the first dt.
-static int init_case_from_pinned(gd2d_handle *h, int32_t icase, double t0, bool nodes_from_cells) {
-    HostCase &hc = h->cases[icase];
-    cudaSetDevice(h->device);
+// Where the primitives of a case are written before its initialisation:
+// FP64, the current primitive buffer; mixed, U, which the init kernel turns
+// into conservatives while writing the FP32 primitives.
+static int case_prims_dst(gd2d_handle *h, int32_t icase, double4 **dst) {
+    const HostCase &hc = h->cases[icase];
     int par = 0;
     int rc = copy_sync(h, &par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost);
     if (rc) return rc;
-    // FP64: the primitives go to the current buffer; mixed: to U, which the
-    // init kernel turns into conservatives while writing the FP32 primitives
-    double4 *dst = h->mixed ? h->s.U + hc.cell_off : h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off;
-    CUDA_TRY(h, cudaMemcpyAsync(dst, h->pinned, sizeof(double4) * hc.nc, cudaMemcpyHostToDevice, h->stream));
+    *dst = h->mixed ? h->s.U + hc.cell_off : h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off;
+    return GD2D_OK;
+}
+
+// The case's primitives, already in place (case_prims_dst), become its
+// state: U, the node fields and the first dt.
+static int init_case(gd2d_handle *h, int32_t icase, double t0, bool nodes_from_cells) {
+    HostCase &hc = h->cases[icase];
     CaseState &cs = h->cs_host[icase];
     cs = CaseState{};
     cs.t = t0;
@@ -899,29 +919,31 @@ int gd2d_set_state(gd2d_handle *h, int32_t icase, const double *density, const d
     int rc = ensure_case(h, icase);
     if (rc) return rc;
     if (!density || !ux || !uy || !pressure) return fail(h, GD2D_ERR_ARG, "NULL field pointer");
-    HostCase &hc = h->cases[icase];
-    double4 *pr = h->pinned;
-    for (int64_t j = 0; j < hc.nc; ++j) {
-        int64_t i = hc.cell_perm[j];
-        pr[j] = make_double4(density[i], ux[i], uy[i], pressure[i]);
-    }
-    return init_case_from_pinned(h, icase, hc.start_time, hc.params.init_nodes != 0);
+    cudaSetDevice(h->device);
+    const HostCase &hc = h->cases[icase];
+    double4 *dst = nullptr;
+    if ((rc = case_prims_dst(h, icase, &dst))) return rc;
+    const int64_t n = hc.nc;
+    double *st = h->d_stage;
+    const double *cols[4] = {density, ux, uy, pressure};
+    for (int v = 0; v < 4; ++v)
+        CUDA_TRY(h, cudaMemcpyAsync(st + v * n, cols[v], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, launch_cols_to_dev(st, h->d_perm + hc.cell_off, n, dst, h->stream));
+    return init_case(h, icase, hc.start_time, hc.params.init_nodes != 0);
 }
 
 int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, double flow_time, int32_t rebuild_nodes) {
     int rc = ensure_case(h, icase);
     if (rc) return rc;
     if (!ucons) return fail(h, GD2D_ERR_ARG, "NULL ucons");
-    HostCase &hc = h->cases[icase];
-    const double G = hc.params.Gamma;
-    double4 *pr = h->pinned;
-    for (int64_t j = 0; j < hc.nc; ++j) {
-        int64_t i = hc.cell_perm[j];
-        double U1 = ucons[cidx(hc.nc, i, 0)], U2 = ucons[cidx(hc.nc, i, 1)], U3 = ucons[cidx(hc.nc, i, 2)],
-               U4 = ucons[cidx(hc.nc, i, 3)];
-        pr[j] = make_double4(U1, U2 / U1, U3 / U1, (G - 1.0) * (U4 - 0.5 * (U2 * U2 + U3 * U3) / U1));
-    }
-    return init_case_from_pinned(h, icase, flow_time, rebuild_nodes != 0);
+    cudaSetDevice(h->device);
+    const HostCase &hc = h->cases[icase];
+    double4 *dst = nullptr;
+    if ((rc = case_prims_dst(h, icase, &dst))) return rc;
+    const int64_t n = hc.nc;
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, ucons, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(h, launch_cons_to_prims(h->d_stage, h->d_perm + hc.cell_off, n, hc.params.Gamma, dst, h->stream));
+    return init_case(h, icase, flow_time, rebuild_nodes != 0);
 }
 
 static int64_t kernels_per_step(const gd2d_handle *h) {
@@ -1106,6 +1128,18 @@ int gd2d_get_history(gd2d_handle *h, int32_t icase, gd2d_stats *out, int32_t cap
     return n;
 }
 
+// One device-order field of a case, reordered on the device into the
+// staging columns and copied to a column-major host matrix.
+static int download_rows(gd2d_handle *h, const double4 *src, const float4 *srcf, const int32_t *inv, int64_t n,
+                         double *dst) {
+    if (!dst) return GD2D_OK;
+    CUDA_TRY(h, srcf ? launch_dev_to_cols_f(srcf, inv, n, h->d_stage, h->stream)
+                     : launch_dev_to_cols(src, inv, n, h->d_stage, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(dst, h->d_stage, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    return GD2D_OK;
+}
+
 int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, double *node_prims) {
     int rc = ensure_case(h, icase);
     if (rc) return rc;
@@ -1114,57 +1148,16 @@ int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, 
     int par = 0;
     rc = copy_sync(h, &par, h->s.parity, sizeof(int), cudaMemcpyDeviceToHost);
     if (rc) return rc;
-    double4 *tmp = h->pinned;
-    if (ucons) {
-        rc = copy_sync(h, tmp, h->s.U + hc.cell_off, sizeof(double4) * hc.nc, cudaMemcpyDeviceToHost);
-        if (rc) return rc;
-        for (int64_t j = 0; j < hc.nc; ++j) {
-            int64_t i = hc.cell_perm[j];
-            ucons[cidx(hc.nc, i, 0)] = tmp[j].x; ucons[cidx(hc.nc, i, 1)] = tmp[j].y;
-            ucons[cidx(hc.nc, i, 2)] = tmp[j].z; ucons[cidx(hc.nc, i, 3)] = tmp[j].w;
-        }
-    }
-    if (prims && h->mixed) {
-        float4 *tf = reinterpret_cast<float4 *>(h->pinned);
-        rc = copy_sync(h, tf, h->s.primf + (int64_t)par * h->m.Nc + hc.cell_off, sizeof(float4) * hc.nc,
-                       cudaMemcpyDeviceToHost);
-        if (rc) return rc;
-        for (int64_t j = 0; j < hc.nc; ++j) {
-            int64_t i = hc.cell_perm[j];
-            prims[cidx(hc.nc, i, 0)] = tf[j].x; prims[cidx(hc.nc, i, 1)] = tf[j].y;
-            prims[cidx(hc.nc, i, 2)] = tf[j].z; prims[cidx(hc.nc, i, 3)] = tf[j].w;
-        }
-        prims = nullptr;
-    }
-    if (node_prims && h->mixed) {
-        float4 *tf = reinterpret_cast<float4 *>(h->pinned);
-        rc = copy_sync(h, tf, h->s.nodePf + hc.node_off, sizeof(float4) * hc.nn, cudaMemcpyDeviceToHost);
-        if (rc) return rc;
-        for (int64_t j = 0; j < hc.nn; ++j) {
-            int64_t J = hc.node_perm[j];
-            node_prims[cidx(hc.nn, J, 0)] = tf[j].x; node_prims[cidx(hc.nn, J, 1)] = tf[j].y;
-            node_prims[cidx(hc.nn, J, 2)] = tf[j].z; node_prims[cidx(hc.nn, J, 3)] = tf[j].w;
-        }
-        node_prims = nullptr;
-    }
-    if (prims) {
-        rc = copy_sync(h, tmp, h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, sizeof(double4) * hc.nc,
-                       cudaMemcpyDeviceToHost);
-        if (rc) return rc;
-        for (int64_t j = 0; j < hc.nc; ++j) {
-            int64_t i = hc.cell_perm[j];
-            prims[cidx(hc.nc, i, 0)] = tmp[j].x; prims[cidx(hc.nc, i, 1)] = tmp[j].y;
-            prims[cidx(hc.nc, i, 2)] = tmp[j].z; prims[cidx(hc.nc, i, 3)] = tmp[j].w;
-        }
-    }
-    if (node_prims) {
-        rc = copy_sync(h, tmp, h->s.nodeP + hc.node_off, sizeof(double4) * hc.nn, cudaMemcpyDeviceToHost);
-        if (rc) return rc;
-        for (int64_t j = 0; j < hc.nn; ++j) {
-            int64_t J = hc.node_perm[j];
-            node_prims[cidx(hc.nn, J, 0)] = tmp[j].x; node_prims[cidx(hc.nn, J, 1)] = tmp[j].y;
-            node_prims[cidx(hc.nn, J, 2)] = tmp[j].z; node_prims[cidx(hc.nn, J, 3)] = tmp[j].w;
-        }
+    const int32_t *inv = h->d_inv + hc.ref_off, *ninv = h->d_ninv + hc.nref_off;
+    if ((rc = download_rows(h, h->s.U + hc.cell_off, nullptr, inv, hc.nc, ucons))) return rc;
+    if (h->mixed) {
+        if ((rc = download_rows(h, nullptr, h->s.primf + (int64_t)par * h->m.Nc + hc.cell_off, inv, hc.nc, prims)))
+            return rc;
+        if ((rc = download_rows(h, nullptr, h->s.nodePf + hc.node_off, ninv, hc.nn, node_prims))) return rc;
+    } else {
+        if ((rc = download_rows(h, h->s.prim + (int64_t)par * h->m.Nc + hc.cell_off, nullptr, inv, hc.nc, prims)))
+            return rc;
+        if ((rc = download_rows(h, h->s.nodeP + hc.node_off, nullptr, ninv, hc.nn, node_prims))) return rc;
     }
     return GD2D_OK;
 }
@@ -1186,17 +1179,8 @@ static int split_buffers(gd2d_handle *h) {
 // A per-cell double4 field of one case to an (nCells x 4) column-major host
 // matrix in reference order.
 static int download_cells(gd2d_handle *h, int32_t icase, const double4 *src, double *dst) {
-    if (!dst) return GD2D_OK;
-    HostCase &hc = h->cases[icase];
-    int rc = copy_sync(h, h->pinned, src + hc.cell_off, sizeof(double4) * hc.nc, cudaMemcpyDeviceToHost);
-    if (rc) return rc;
-    const double4 *t = h->pinned;
-    for (int64_t j = 0; j < hc.nc; ++j) {
-        int64_t i = hc.cell_perm[j];
-        dst[cidx(hc.nc, i, 0)] = t[j].x; dst[cidx(hc.nc, i, 1)] = t[j].y;
-        dst[cidx(hc.nc, i, 2)] = t[j].z; dst[cidx(hc.nc, i, 3)] = t[j].w;
-    }
-    return GD2D_OK;
+    const HostCase &hc = h->cases[icase];
+    return download_rows(h, src + hc.cell_off, nullptr, h->d_inv + hc.ref_off, hc.nc, dst);
 }
 
 int gd2d_calc_one_stage(gd2d_handle *h, int32_t icase, double beta, double dt, double flow_time, double *fluxes,
@@ -1428,7 +1412,6 @@ int gd2d_destroy(gd2d_handle *h) {
     drop_graph(h);
     for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
     for (auto &e : h->ev_eager) if (e) cudaEventDestroy(e);
-    if (h->pinned) cudaFreeHost(h->pinned);
     if (h->ring_host) cudaFreeHost(h->ring_host);
     h->buf.free_all();
     if (h->own_stream) cudaStreamDestroy(h->stream);

@@ -174,6 +174,14 @@ cudaError_t launch_cell_step_f64(const DevMesh &m, const DevState &s, int flux, 
                                  const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_cell_step_tf_f64(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
                                     const LaunchCfg &lc, cudaStream_t st);
+// Reordering between the reference's column-major rows and device order
+// (cols: [n x 4] column-major; perm[j] = reference row of device record j;
+// inv[i] = device record of reference row i).
+cudaError_t launch_cols_to_dev(const double *cols, const int32_t *perm, int64_t n, double4 *dst, cudaStream_t st);
+cudaError_t launch_cons_to_prims(const double *cols, const int32_t *perm, int64_t n, double gamma, double4 *dst,
+                                 cudaStream_t st);
+cudaError_t launch_dev_to_cols(const double4 *src, const int32_t *inv, int64_t n, double *cols, cudaStream_t st);
+cudaError_t launch_dev_to_cols_f(const float4 *src, const int32_t *inv, int64_t n, double *cols, cudaStream_t st);
 cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, bool flip_parity,
                                 bool zero_prims, int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);

@@ -141,3 +141,86 @@ cudaError_t launch_diff_only_f64(const DevMesh &m, const DevState &s, double4 *d
 }
 
 }  // namespace gd2d
+
+// ------------------------------------------ reference order <-> device order
+//
+// Fields cross the ABI in the reference's layout: column-major [n x 4]
+// matrices (or four columns) indexed by the reference's cell / node ids.
+// These kernels do the reordering on the device, so the host only copies
+// contiguous blocks (a permutation on the host is a cache miss per value).
+
+namespace gd2d {
+
+namespace {
+
+int reorder_grid(int64_t n) {
+    int64_t g = (n + 255) / 256;
+    if (g < 1) g = 1;
+    if (g > 148LL * 32) g = 148 * 32;
+    return (int)g;
+}
+
+// dst[j] = (a[i], b[i], c[i], d[i]) with i = perm[j]: reference rows to
+// device-order records.
+__global__ void __launch_bounds__(256) k_cols_to_dev(const double *__restrict__ a, const double *__restrict__ b,
+                                                     const double *__restrict__ c, const double *__restrict__ d,
+                                                     const int32_t *__restrict__ perm, int64_t n,
+                                                     double4 *__restrict__ dst) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = perm[j];
+        dst[j] = make_double4(a[i], b[i], c[i], d[i]);
+    }
+}
+
+// Conservative reference rows to device-order primitives, the formula of
+// the primitives recovery (evaluate2d.jl:87-104) in the same order; this
+// translation unit has no multiply-add contraction, like the host code it
+// replaces.
+__global__ void __launch_bounds__(256) k_cons_to_prims(const double *__restrict__ u, int64_t n,
+                                                       const int32_t *__restrict__ perm, double G,
+                                                       double4 *__restrict__ dst) {
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = perm[j];
+        const double U1 = u[i], U2 = u[i + n], U3 = u[i + 2 * n], U4 = u[i + 3 * n];
+        dst[j] = make_double4(U1, U2 / U1, U3 / U1, (G - 1.0) * (U4 - 0.5 * (U2 * U2 + U3 * U3) / U1));
+    }
+}
+
+// dst[i + v n] = component v of src[inv[i]]: device-order records to
+// reference-order columns (FP32 records widened exactly).
+template <class T4>
+__global__ void __launch_bounds__(256) k_dev_to_cols(const T4 *__restrict__ src, const int32_t *__restrict__ inv,
+                                                     int64_t n, double *__restrict__ dst) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const T4 r = src[inv[i]];
+        dst[i] = (double)r.x;
+        dst[i + n] = (double)r.y;
+        dst[i + 2 * n] = (double)r.z;
+        dst[i + 3 * n] = (double)r.w;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_cols_to_dev(const double *cols, const int32_t *perm, int64_t n, double4 *dst, cudaStream_t st) {
+    k_cols_to_dev<<<reorder_grid(n), 256, 0, st>>>(cols, cols + n, cols + 2 * n, cols + 3 * n, perm, n, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cons_to_prims(const double *cols, const int32_t *perm, int64_t n, double gamma, double4 *dst,
+                                 cudaStream_t st) {
+    k_cons_to_prims<<<reorder_grid(n), 256, 0, st>>>(cols, n, perm, gamma, dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dev_to_cols(const double4 *src, const int32_t *inv, int64_t n, double *cols, cudaStream_t st) {
+    k_dev_to_cols<double4><<<reorder_grid(n), 256, 0, st>>>(src, inv, n, cols);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dev_to_cols_f(const float4 *src, const int32_t *inv, int64_t n, double *cols, cudaStream_t st) {
+    k_dev_to_cols<float4><<<reorder_grid(n), 256, 0, st>>>(src, inv, n, cols);
+    return cudaGetLastError();
+}
+
+}  // namespace gd2d
