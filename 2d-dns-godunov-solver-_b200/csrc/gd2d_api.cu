@@ -14,6 +14,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/godunov2d.h"
@@ -86,6 +87,7 @@ struct gd2d_handle {
     int32_t *d_inv = nullptr;    // [sum nc] device cell of each reference row
     int32_t *d_ninv = nullptr;   // [sum nn] device node of each reference node
     double *d_stage = nullptr;   // [4 x max(nc, nn)] reference-order columns in transit
+    double *h_stage = nullptr;   // page-locked host copy of d_stage
     // face-loop variants: faces sorted by colour, colour ranges, flux storage
     int loop = GD2D_LOOP_CELL;
     int4 *d_faces = nullptr;
@@ -699,6 +701,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     auto bail = [&](int rc) {
         h->buf.free_all();
         if (h->ring_host) cudaFreeHost(h->ring_host);
+        if (h->h_stage) cudaFreeHost(h->h_stage);
         for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
         for (auto &e : h->ev_eager) if (e) cudaEventDestroy(e);
         if (h->own_stream) cudaStreamDestroy(h->stream);
@@ -825,6 +828,8 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         ALLOC(h->d_inv, inv.size()); UPLOAD(h->d_inv, inv);
         ALLOC(h->d_ninv, ninv.size()); UPLOAD(h->d_ninv, ninv);
         ALLOC(h->d_stage, (size_t)4 * maxrows);
+        cudaError_t e = cudaMallocHost((void **)&h->h_stage, sizeof(double) * 4 * (size_t)maxrows);
+        if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaMallocHost: %s", cudaGetErrorString(e)));
     }
 #undef ALLOC
 #undef UPLOAD
@@ -859,6 +864,28 @@ static int copy_sync(gd2d_handle *h, void *dst, const void *src, size_t bytes, c
     CUDA_TRY(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return GD2D_OK;
+}
+
+// Host copy between a caller's array and the page-locked stage, split over
+// a few threads for large fields (one thread leaves most of the memory
+// bandwidth unused).
+static void host_copy(void *dst, const void *src, size_t bytes) {
+    const size_t kPart = (size_t)4 << 20;
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = std::max(1u, std::min(nt, 8u));
+    nt = (unsigned)std::min<size_t>(nt, std::max<size_t>(1, bytes / kPart));
+    if (nt <= 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t part = (bytes + nt - 1) / nt;
+    for (unsigned k = 0; k < nt; ++k) {
+        const size_t b0 = k * part, b1 = std::min(bytes, b0 + part);
+        if (b0 >= b1) break;
+        th.emplace_back([=] { std::memcpy((char *)dst + b0, (const char *)src + b0, b1 - b0); });
+    }
+    for (auto &t : th) t.join();
 }
 
 static int ensure_case(gd2d_handle *h, int32_t icase) {
@@ -926,8 +953,8 @@ int gd2d_set_state(gd2d_handle *h, int32_t icase, const double *density, const d
     const int64_t n = hc.nc;
     double *st = h->d_stage;
     const double *cols[4] = {density, ux, uy, pressure};
-    for (int v = 0; v < 4; ++v)
-        CUDA_TRY(h, cudaMemcpyAsync(st + v * n, cols[v], sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    for (int v = 0; v < 4; ++v) host_copy(h->h_stage + v * n, cols[v], sizeof(double) * n);
+    CUDA_TRY(h, cudaMemcpyAsync(st, h->h_stage, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, launch_cols_to_dev(st, h->d_perm + hc.cell_off, n, dst, h->stream));
     return init_case(h, icase, hc.start_time, hc.params.init_nodes != 0);
 }
@@ -941,7 +968,8 @@ int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, do
     double4 *dst = nullptr;
     if ((rc = case_prims_dst(h, icase, &dst))) return rc;
     const int64_t n = hc.nc;
-    CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, ucons, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, h->stream));
+    host_copy(h->h_stage, ucons, sizeof(double) * 4 * n);
+    CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, h->h_stage, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, launch_cons_to_prims(h->d_stage, h->d_perm + hc.cell_off, n, hc.params.Gamma, dst, h->stream));
     return init_case(h, icase, flow_time, rebuild_nodes != 0);
 }
@@ -1135,8 +1163,9 @@ static int download_rows(gd2d_handle *h, const double4 *src, const float4 *srcf,
     if (!dst) return GD2D_OK;
     CUDA_TRY(h, srcf ? launch_dev_to_cols_f(srcf, inv, n, h->d_stage, h->stream)
                      : launch_dev_to_cols(src, inv, n, h->d_stage, h->stream));
-    CUDA_TRY(h, cudaMemcpyAsync(dst, h->d_stage, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    host_copy(dst, h->h_stage, sizeof(double) * 4 * n);
     return GD2D_OK;
 }
 
@@ -1413,6 +1442,7 @@ int gd2d_destroy(gd2d_handle *h) {
     for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
     for (auto &e : h->ev_eager) if (e) cudaEventDestroy(e);
     if (h->ring_host) cudaFreeHost(h->ring_host);
+    if (h->h_stage) cudaFreeHost(h->h_stage);
     h->buf.free_all();
     if (h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
