@@ -914,8 +914,12 @@ static int case_prims_dst(gd2d_handle *h, int32_t icase, double4 **dst) {
 }
 
 // The case's primitives, already in place (case_prims_dst), become its
-// state: U, the node fields and the first dt.
-static int init_case(gd2d_handle *h, int32_t icase, double t0, bool nodes_from_cells) {
+// state: U, the node fields and the first dt.  With `exact_cons` (reference
+// order columns on the device) U is then overwritten by those conservatives,
+// before the node pass, so that a restart continues bit for bit (the
+// round trip conservatives -> primitives -> conservatives is inexact).
+static int init_case(gd2d_handle *h, int32_t icase, double t0, bool nodes_from_cells,
+                     const double *exact_cons = nullptr) {
     HostCase &hc = h->cases[icase];
     CaseState &cs = h->cs_host[icase];
     cs = CaseState{};
@@ -925,10 +929,14 @@ static int init_case(gd2d_handle *h, int32_t icase, double t0, bool nodes_from_c
     const DevCase &d = h->hcases[icase];
     if (h->mixed) {
         CUDA_TRY(h, launch_init_state_mixed(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
+        if (exact_cons)
+            CUDA_TRY(h, launch_cols_to_dev(exact_cons, h->d_perm + hc.cell_off, hc.nc, h->s.U + hc.cell_off, h->stream));
         CUDA_TRY(h, launch_node_avg_mixed(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off,
                                           hc.node_off + hc.nn, h->lc, h->stream));
     } else {
         CUDA_TRY(h, launch_init_state_f64(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
+        if (exact_cons)
+            CUDA_TRY(h, launch_cols_to_dev(exact_cons, h->d_perm + hc.cell_off, hc.nc, h->s.U + hc.cell_off, h->stream));
         CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off,
                                         hc.node_off + hc.nn, h->lc, h->stream));
     }
@@ -971,7 +979,7 @@ int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, do
     host_copy(h->h_stage, ucons, sizeof(double) * 4 * n);
     CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, h->h_stage, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, h->stream));
     CUDA_TRY(h, launch_cons_to_prims(h->d_stage, h->d_perm + hc.cell_off, n, hc.params.Gamma, dst, h->stream));
-    return init_case(h, icase, flow_time, rebuild_nodes != 0);
+    return init_case(h, icase, flow_time, rebuild_nodes != 0, h->d_stage);
 }
 
 static int64_t kernels_per_step(const gd2d_handle *h) {

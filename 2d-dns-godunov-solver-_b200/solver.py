@@ -103,6 +103,7 @@ class Solver:
         self._views = (N.MeshView * n)(*[mesh_view(m) for m in self.meshes])
         self._params = (N.Params * n)(*[make_params(c) for c in self.cfgs])
         self._launch = launch if launch is not None else make_launch()
+        self._t0 = [0.0] * n
         h = C.c_void_p()
         N.check(self.L.gd2d_setup(C.byref(h), n, self._views, self._params, C.byref(self._launch)))
         self.h = h
@@ -133,6 +134,7 @@ class Solver:
                 raise ValueError("field size does not match the mesh")
         dp = C.POINTER(C.c_double)
         self._chk(self.L.gd2d_set_state(self.h, icase, *[a.ctypes.data_as(dp) for a in arrs]))
+        self._t0[icase] = float(self.cfgs[icase].get("start_time", 0.0))
 
     set_state = createFields2d
 
@@ -140,6 +142,37 @@ class Solver:
         u = np.asfortranarray(ucons, dtype=np.float64)
         self._chk(self.L.gd2d_set_conservative(self.h, icase, u.ctypes.data_as(C.POINTER(C.c_double)),
                                                float(flow_time), int(rebuild_nodes)))
+        self._t0[icase] = float(flow_time)
+
+    def flow_time(self, icase: int) -> float:
+        """Current flowTime of a case: its start (set_state / restart) plus
+        the dt of every step taken since."""
+        h = self.history(icase, 1)
+        return h[-1]["flowTime"] + h[-1]["dt"] if h else self._t0[icase]
+
+    def save_snapshot(self, icase: int, path: str) -> None:
+        """Solution snapshot of one case as a raw .npz (no VTK): the
+        reference's solutionCellsT fields (flowTime, dt, densityCells,
+        UxCells, UyCells, pressureCells; primeObjects.jl:197-205,
+        evaluate2d.jl:187-203) plus the conservative state, which makes a
+        restart continue bit for bit."""
+        st = self.get_state(icase)
+        h = self.history(icase, 1)
+        P = st["prims"]
+        np.savez(path, flowTime=self.flow_time(icase), dt=(h[-1]["dt"] if h else 0.0),
+                 densityCells=P[:, 0], UxCells=P[:, 1], UyCells=P[:, 2], pressureCells=P[:, 3],
+                 Ucons=st["Ucons"], nCells=self.meshes[icase].nCells)
+
+    def load_snapshot(self, icase: int, path: str) -> float:
+        """Restart a case from save_snapshot's file (loadPrevResults.jl:3-38
+        reads the primitives; here the conservatives are restored exactly and
+        the node values rebuilt from them).  Returns the restored flowTime."""
+        d = np.load(path)
+        if int(d["nCells"]) != self.meshes[icase].nCells:
+            raise ValueError("snapshot does not match the case's mesh")
+        t = float(d["flowTime"])
+        self.set_conservative(icase, np.asfortranarray(d["Ucons"]), t, rebuild_nodes=True)
+        return t
 
     # -- stepping ------------------------------------------------------------
     def propagate2d(self, nsteps: int) -> List[Dict]:

@@ -22,6 +22,7 @@ import argparse
 import json
 import math
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -175,27 +176,57 @@ def dist_barrier(dist):
         dist.barrier()
 
 
-def cpu_reference(pkg, items, steps, warmup, budget_s=25.0):
-    """Time the CPU restatement of the reference step (oracle, all host
-    threads) on a bounded sample of the workload."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor() or "unknown"
+
+
+def cpu_reference(pkg, items, steps, warmup, budget_s=25.0, single_thread_s=8.0):
+    """Time the CPU restatement of the reference step (oracle) on a bounded
+    sample of the workload: all host threads, one warm-up step, then five
+    timed repeats of equal length (median reported); plus a one-thread
+    figure on a step or two."""
     from oracle import oracle as orc
     orc.build()
     nthreads = os.cpu_count() or 1
     mesh, cfg, prims = items[0]
+    cells = mesh.nCells
     o = orc.Oracle(mesh, cfg, nthreads=nthreads)
     o.init_fields(*prims)
     t0 = time.perf_counter()
     o.step()
     t1 = time.perf_counter() - t0
-    nsteps = max(1, min(steps, int(budget_s / max(t1, 1e-6))))
-    t0 = time.perf_counter()
-    for _ in range(nsteps):
-        o.step()
-    dt = time.perf_counter() - t0
-    cells = mesh.nCells
-    return {"value": cells * nsteps / dt / 1e6, "unit": "Mcell-steps/s", "cores": nthreads, "kind": "port",
-            "sample": f"{nsteps} steps of case 0 ({cells} cells) after 1 warm-up step, {nthreads} threads",
-            "seconds": dt}
+    reps = 5
+    per_rep = max(1, min(steps, int(budget_s / reps / max(t1, 1e-6))))
+    rates = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        for _ in range(per_rep):
+            o.step()
+        rates.append(cells * per_rep / (time.perf_counter() - t0) / 1e6)
+    rates.sort()
+    single = None
+    if single_thread_s > 0:
+        o1 = orc.Oracle(mesh, cfg, nthreads=1)
+        o1.init_fields(*prims)
+        t0 = time.perf_counter()
+        o1.step()
+        ts = time.perf_counter() - t0
+        n1 = max(1, min(3, int(single_thread_s / max(ts, 1e-6))))
+        t0 = time.perf_counter()
+        for _ in range(n1):
+            o1.step()
+        single = cells * n1 / (time.perf_counter() - t0) / 1e6
+    return {"value": rates[len(rates) // 2], "unit": "Mcell-steps/s", "cores": nthreads, "kind": "port",
+            "sample": f"median of {reps} repeats of {per_rep} steps of case 0 ({cells} cells) after 1 warm-up "
+                      f"step, {nthreads} threads",
+            "repeats": [round(r, 4) for r in rates], "single_thread_value": single, "host": cpu_model()}
 
 
 def mixed_variant(pkg, items, s64, args, peak):
@@ -279,7 +310,8 @@ def main():
         line = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": cb["unit"], "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg_line,
-                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "repeats",
+                                                    "single_thread_value", "host")},
                 "e2e": {"value": cb["value"], "unit": cb["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         dist_barrier(dist)
@@ -357,7 +389,8 @@ def main():
         line["mixed"] = mixed_variant(pkg, items, s, args, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(pkg, items, args.steps, args.warmup)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "repeats",
+                                                   "single_thread_value", "host")}
     if rank == 0:
         print(json.dumps(line), flush=True)
     s.close()

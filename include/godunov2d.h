@@ -166,8 +166,11 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
 int gd2d_set_state(gd2d_handle *h, int32_t icase, const double *density, const double *ux,
                    const double *uy, const double *pressure);
 
-/* Restart from a conservative state (nCells x 4) and time; node primitives
- * are rebuilt from it (loadPrevResults.jl:3-38). */
+/* Restart from a conservative state (nCells x 4) and time
+ * (loadPrevResults.jl:3-38): U is kept exactly, the primitives, the next dt
+ * and (rebuild_nodes != 0) the node values are recomputed from it as a step
+ * would, so an FP64 run restarted from gd2d_get_state's Ucons and its
+ * flowTime continues bit for bit. */
 int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, double flow_time,
                           int32_t rebuild_nodes);
 
