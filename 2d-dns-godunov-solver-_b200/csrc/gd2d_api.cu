@@ -355,7 +355,9 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         return fail(nullptr, GD2D_ERR_ARG, "block must be 128 or 256");
     }
     h->lc.block = block;
-    h->lc.node_block = h->launch.node_block ? h->launch.node_block : 256;
+    // node-side passes: 64-thread blocks measured fastest (finer-grained
+    // scheduling of their gathers; 2% of the step on the 2.09M-cell cylinder)
+    h->lc.node_block = h->launch.node_block ? h->launch.node_block : 64;
     if (h->lc.node_block != 64 && h->lc.node_block != 128 && h->lc.node_block != 256) {
         delete h;
         return fail(nullptr, GD2D_ERR_ARG, "node_block must be 64, 128 or 256");

@@ -146,9 +146,9 @@ __global__ void __launch_bounds__(256, 6) k_node_avg_mixed(const DevMesh m, cons
 template <bool QUAD>
 __global__ void __launch_bounds__(256, 6) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
-        const int4 nb = m.nbr[g];
-        if (nb.x == kAbsent) continue;
-        const int nf = (QUAD && nb.w != kAbsent) ? 4 : 3;
+        // padding cells have zero area; triangles a zero-length fourth edge
+        if (m.areaf[g] == 0.f) continue;
+        const int nf = (QUAD && m.lenf[3 * m.Nc + g] != 0.f) ? 4 : 3;
         float sx[3] = {0.f, 0.f, 0.f}, sy[3] = {0.f, 0.f, 0.f};
         for (int k = 0; k < nf; ++k) {
             const int64_t o = (int64_t)k * m.Nc + g;

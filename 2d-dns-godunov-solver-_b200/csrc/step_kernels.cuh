@@ -571,9 +571,11 @@ __global__ void __launch_bounds__(256, 4) k_node_avg(const DevMesh m, const DevS
 template <bool QUAD>
 __global__ void __launch_bounds__(256, 4) k_grad1_cells(const DevMesh m, const DevState s) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
-        const int4 nb = m.nbr[g];
-        if (nb.x == kAbsent) continue;
-        const int nf = (QUAD && nb.w != kAbsent) ? 4 : 3;
+        // padding cells have zero area (real ones are validated positive);
+        // a triangle's fourth edge has zero length: no neighbour table read
+        const double area = m.area[g];
+        if (area == 0.0) continue;
+        const int nf = (QUAD && m.len[3 * m.Nc + g] != 0.0) ? 4 : 3;
         double sx[3] = {0.0, 0.0, 0.0}, sy[3] = {0.0, 0.0, 0.0};
         for (int k = 0; k < nf; ++k) {
             const int64_t o = (int64_t)k * m.Nc + g;
@@ -588,7 +590,6 @@ __global__ void __launch_bounds__(256, 4) k_grad1_cells(const DevMesh m, const D
             fx = 0.5 * (A.z + B.z) * -ny * side; fy = 0.5 * (A.z + B.z) * -nx * side;
             sx[2] = (k == 0) ? fx : sx[2] + fx; sy[2] = (k == 0) ? fy : sy[2] + fy;
         }
-        const double area = m.area[g];
         NodeGrad r;
         r.ru = make_double2(sx[0] / area, sy[0] / area);
         r.rv = make_double2(sx[1] / area, sy[1] / area);
