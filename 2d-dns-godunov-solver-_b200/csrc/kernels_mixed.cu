@@ -14,7 +14,7 @@ namespace {
 
 template <int FLUX, bool VISC, bool QUAD, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, const DevState s) {
-    __shared__ Part sh[8];
+    __shared__ double s_red[kPartFields * 256];
     const int par = *s.parity;
     const float4 *__restrict__ pin = s.primf + (int64_t)par * m.Nc;
     float4 *__restrict__ pout = s.primf + (int64_t)(par ^ 1) * m.Nc;
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
             if (VISC) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update_mixed(m, s, P, g, me, F, diff, dt, pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, sh, false);
+        tile_epilogue(m, s, tile, c, part, s_red, false);
     }
 }
 
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(256, 6) k_grad1_nodes_mixed(const DevMesh m, c
 // U holds FP64 primitives on entry: conservatives (utilsFVM2dp.jl:4-17) and
 // the FP32 primitives are written, with the first dt's reductions.
 __global__ void __launch_bounds__(256) k_init_state_mixed(const DevMesh m, const DevState s, int64_t t0, int64_t t1) {
-    __shared__ Part sh[8];
+    __shared__ double s_red[kPartFields * 256];
     const int par = *s.parity;
     float4 *__restrict__ pout = s.primf + (int64_t)par * m.Nc;
     for (int64_t tile = t0 + blockIdx.x; tile < t1; tile += gridDim.x) {
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(256) k_init_state_mixed(const DevMesh m, const
             part.vmax = vmax;
             part.rmin = (double)m.charlenf[g] / vmax;
         }
-        tile_epilogue(m, s, tile, c, part, sh, true);
+        tile_epilogue(m, s, tile, c, part, s_red, true);
     }
 }
 

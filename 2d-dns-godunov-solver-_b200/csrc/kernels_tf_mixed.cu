@@ -14,10 +14,15 @@ namespace {
 template <int FLUX, bool VISC, bool QUAD, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh m, const DevState s) {
     constexpr int NS = QUAD ? 4 : 3;
-    __shared__ Part sh[8];
-    __shared__ float4 s_prim[256];
+    // one buffer for the step reduction; the tile's primitives and flux
+    // slots live in it until the reduction retires them
+    // declared as double4 for its 32-byte alignment (float4 views need 16)
+    __shared__ double4 s_buf[kPartFields * 256 / 4];
     __shared__ float s_hx[256];
-    __shared__ float4 s_flux[NS][256];
+    static_assert((1 + NS) * 256 * 16 <= kPartFields * 256 * 8, "tile buffers");
+    double *const s_red = reinterpret_cast<double *>(s_buf);
+    float4 *const s_prim = reinterpret_cast<float4 *>(s_buf);
+    float4 (*const s_flux)[256] = reinterpret_cast<float4 (*)[256]>(s_prim + 256);
     const int par = *s.parity;
     const float4 *__restrict__ pin = s.primf + (int64_t)par * m.Nc;
     float4 *__restrict__ pout = s.primf + (int64_t)(par ^ 1) * m.Nc;
@@ -85,7 +90,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
             }
             cell_update_mixed(m, s, P, g, me, F, diff, dt, pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, sh, false);
+        tile_epilogue(m, s, tile, c, part, s_red, false);
     }
 }
 

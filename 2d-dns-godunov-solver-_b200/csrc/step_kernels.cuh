@@ -37,19 +37,11 @@ struct Part {
         rhomax = fmax(rhomax, o.rhomax);
         bad = fmax(bad, o.bad);
     }
-    __device__ void shfl_down(int off) {
-        Part o;
-        for (int v = 0; v < 4; ++v) {
-            o.res[v] = __shfl_down_sync(0xffffffffu, res[v], off);
-            o.tot[v] = __shfl_down_sync(0xffffffffu, tot[v], off);
-        }
-        o.ek = __shfl_down_sync(0xffffffffu, ek, off);
-        o.vmax = __shfl_down_sync(0xffffffffu, vmax, off);
-        o.rmin = __shfl_down_sync(0xffffffffu, rmin, off);
-        o.rhomin = __shfl_down_sync(0xffffffffu, rhomin, off);
-        o.rhomax = __shfl_down_sync(0xffffffffu, rhomax, off);
-        o.bad = __shfl_down_sync(0xffffffffu, bad, off);
-        combine(o);
+    // field f at p[f * stride], in record order
+    __device__ void store_strided(double *p, int stride) const {
+        for (int v = 0; v < 4; ++v) { p[(P_RES0 + v) * stride] = res[v]; p[(P_TOT0 + v) * stride] = tot[v]; }
+        p[P_EK * stride] = ek; p[P_VMAX * stride] = vmax; p[P_RMIN * stride] = rmin;
+        p[P_RHOMIN * stride] = rhomin; p[P_RHOMAX * stride] = rhomax; p[P_BAD * stride] = bad;
     }
     __device__ void store(double *p) const {
         for (int v = 0; v < 4; ++v) { p[P_RES0 + v] = res[v]; p[P_TOT0 + v] = tot[v]; }
@@ -63,36 +55,68 @@ struct Part {
     }
 };
 
-// Deterministic block reduction (fixed tree for a fixed blockDim); the
-// result is valid in thread 0.  `sh` holds blockDim/32 records.
-__device__ __forceinline__ void block_reduce(Part &p, Part *sh) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int off = 16; off > 0; off >>= 1) p.shfl_down(off);
-    if (lane == 0) sh[warp] = p;
-    __syncthreads();
-    if (warp == 0) {
-        if (lane < nw) p = sh[lane];
-        else p.init();
-        for (int off = 16; off > 0; off >>= 1) p.shfl_down(off);
-    }
-    __syncthreads();
+// Fields of a Part in record order; 0-8 are sums, then max, min, min, max, max.
+constexpr int kPartFields = 14;
+__device__ __forceinline__ double part_op(int f, double a, double b) {
+    if (f < 9) return a + b;
+    return (f == 10 || f == 11) ? fmin(a, b) : fmax(a, b);
 }
 
-// Per-case finalization by the block that completed the case's last tile
+// Field f of a Part (record order).
+__device__ __forceinline__ double part_get(const Part &p, int f) {
+    switch (f) {
+    case 0: case 1: case 2: case 3: return p.res[f];
+    case 4: case 5: case 6: case 7: return p.tot[f - 4];
+    case 8: return p.ek;
+    case 9: return p.vmax;
+    case 10: return p.rmin;
+    case 11: return p.rhomin;
+    case 12: return p.rhomax;
+    default: return p.bad;
+    }
+}
+__device__ __forceinline__ void part_set(Part &p, int f, double x) {
+    switch (f) {
+    case 0: case 1: case 2: case 3: p.res[f] = x; break;
+    case 4: case 5: case 6: case 7: p.tot[f - 4] = x; break;
+    case 8: p.ek = x; break;
+    case 9: p.vmax = x; break;
+    case 10: p.rmin = x; break;
+    case 11: p.rhomin = x; break;
+    case 12: p.rhomax = x; break;
+    default: p.bad = x; break;
+    }
+}
+
+// Records [b, e) (kPartials doubles apart) reduced by one warp in a fixed
+// order: lane l folds records b + l, b + l + 32, ..., then a fixed shuffle
+// tree per field.  The result is valid in lane 0.
+__device__ __forceinline__ Part warp_reduce_records(const double *recs, int64_t b, int64_t e) {
+    const int lane = threadIdx.x & 31;
+    Part acc;
+    acc.init();
+    for (int64_t q = b + lane; q < e; q += 32) {
+        Part o;
+        o.load_cg(recs + q * kPartials);
+        acc.combine(o);
+    }
+#pragma unroll
+    for (int f = 0; f < kPartFields; ++f) {
+        double x = part_get(acc, f);
+        for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
+        part_set(acc, f, x);
+    }
+    return acc;
+}
+
+// Per-case finalization by the warp that completed the case's last tile
 // group: reduce the group records in a fixed order, publish the step
 // statistics and advance time (flowTime += dt, testInviscidFluxesGPUx32.jl:401)
 // and the next dt (tau at :322-324, or the local-CFL extension).
-static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c, Part *sh, bool is_init) {
+static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c, bool is_init) {
     const DevCase &P = m.cases[c];
-    Part acc;
-    acc.init();
-    for (int64_t q = P.group_begin + threadIdx.x; q < P.group_end; q += blockDim.x) {
-        Part o;
-        o.load_cg(s.gpart + q * kPartials);
-        acc.combine(o);
-    }
-    block_reduce(acc, sh);
-    if (threadIdx.x == 0) {
+    const Part acc = warp_reduce_records(s.gpart, P.group_begin, P.group_end);
+    if ((threadIdx.x & 31) == 0) {
         CaseState *cs = s.cstate + c;
         double vnew = acc.vmax, rnew = acc.rmin;
         if (!is_init) {
@@ -124,52 +148,62 @@ static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c,
     }
 }
 
-// Publish the tile record; the block that completes a group of kGroupTiles
-// tiles reduces the group (fixed order) into a group record, and the block
-// that completes a case's last group finalizes the case.  Two short levels
-// instead of one long one: the serial tail at the end of the kernel reads
-// at most one record per thread per level.  Whichever block ends up doing
-// a reduction, its order is the same, so the results are deterministic.
+// The tile's reduction record and the step's two-level completion count.
+//
+// Every thread's Part goes to shared memory in a transposed layout (`red`:
+// kPartFields x blockDim doubles; it may alias buffers the block used for
+// the tile, the first barrier retires them).  Warp w reduces fields w, w +
+// nwarps, ... (each lane folds its column in a fixed order, then a fixed
+// shuffle tree), writes them into the tile's record in global memory, and
+// counts itself done for the tile's group.  The warp that completes a group
+// of kGroupTiles tiles reduces the group's records into a group record; the
+// warp that completes a case's last group finalizes the case.  No thread
+// waits on another's atomic; whichever warp ends up doing a reduction, its
+// order is the same, so the results are deterministic.
 __device__ __forceinline__ void tile_epilogue(const DevMesh &m, const DevState &s, int64_t tile, int c, Part &p,
-                                              Part *sh, bool is_init) {
-    __shared__ int s_last_group, s_last_case;
+                                              double *red, bool is_init) {
     const DevCase &P = m.cases[c];
+    const int B = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = B >> 5;
     const int64_t gi = (tile - P.tile_begin) / kGroupTiles;
     const int64_t gid = P.group_begin + gi;
     const int64_t t0 = P.tile_begin + gi * kGroupTiles;
     const int64_t t1 = (t0 + kGroupTiles < P.tile_end) ? t0 + kGroupTiles : P.tile_end;
-    block_reduce(p, sh);
-    if (threadIdx.x == 0) {
-        p.store(s.part + tile * kPartials);
-        __threadfence();
-        const unsigned int prev = atomicAdd(&s.group_done[gid], 1u);
-        s_last_group = (prev == (unsigned int)(t1 - t0) - 1u) ? 1 : 0;
-    }
     __syncthreads();
-    if (s_last_group) {
+    p.store_strided(red + t, B);
+    __syncthreads();
+    double *rec = s.part + tile * kPartials;
+    for (int f = warp; f < kPartFields; f += nw) {
+        const double *row = red + f * B;
+        double x = row[lane];
+        for (int j = lane + 32; j < B; j += 32) x = part_op(f, x, row[j]);
+        for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
+        if (lane == 0) rec[f] = x;  // field f is record slot f
+    }
+    int last = 0;
+    if (lane == 0) {
         __threadfence();
-        Part acc;
-        acc.init();
-        for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
-            Part o;
-            o.load_cg(s.part + t * kPartials);
-            acc.combine(o);
-        }
-        block_reduce(acc, sh);
-        if (threadIdx.x == 0) {
+        const unsigned int need = (unsigned int)((t1 - t0) * nw);
+        last = (atomicAdd(&s.group_done[gid], 1u) == need - 1u) ? 1 : 0;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+        __threadfence();
+        const Part acc = warp_reduce_records(s.part, t0, t1);
+        int last_case = 0;
+        if (lane == 0) {
             acc.store(s.gpart + gid * kPartials);
             s.group_done[gid] = 0u;
             __threadfence();
             const unsigned int ng = (unsigned int)(P.group_end - P.group_begin);
-            const unsigned int prev = atomicAdd(&s.cstate[c].tiles_done, 1u);
-            s_last_case = (prev == ng - 1u) ? 1 : 0;
+            last_case = (atomicAdd(&s.cstate[c].tiles_done, 1u) == ng - 1u) ? 1 : 0;
         }
-        __syncthreads();
-        if (s_last_case) {
+        last_case = __shfl_sync(0xffffffffu, last_case, 0);
+        if (last_case) {
             __threadfence();
-            finalize_case(m, s, c, sh, is_init);
+            finalize_case(m, s, c, is_init);
         }
     }
+    // the next tile may reuse what `red` aliases
     __syncthreads();
 }
 
@@ -352,7 +386,7 @@ __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s,
 
 template <int FLUX, bool VISC, bool QUAD, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const DevState s) {
-    __shared__ Part sh[8];
+    __shared__ double s_red[kPartFields * 256];
     const int par = *s.parity;
     const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
     double4 *__restrict__ pout = s.prim + (int64_t)(par ^ 1) * m.Nc;
@@ -392,7 +426,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const 
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update(m, s, P, g, me, F, diff, dt, pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, sh, false);
+        tile_epilogue(m, s, tile, c, part, s_red, false);
     }
 }
 
@@ -410,10 +444,14 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const 
 template <int FLUX, bool VISC, bool QUAD, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, const DevState s) {
     constexpr int NS = QUAD ? 4 : 3;
-    __shared__ Part sh[8];
-    __shared__ double4 s_prim[256];
+    // one buffer: the tile's primitives, then its flux slots; the step
+    // reduction reuses it once both have been consumed
+    __shared__ double4 s_mem[(1 + NS) * 256];
     __shared__ double s_hx[256];
-    __shared__ double4 s_flux[NS][256];
+    static_assert((1 + NS) * 256 * 4 >= kPartFields * 256, "reduction buffer");
+    double4 *const s_prim = s_mem;
+    double4 (*const s_flux)[256] = reinterpret_cast<double4 (*)[256]>(s_mem + 256);
+    double *const s_red = reinterpret_cast<double *>(s_mem);
     const int par = *s.parity;
     const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
     double4 *__restrict__ pout = s.prim + (int64_t)(par ^ 1) * m.Nc;
@@ -478,7 +516,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
             }
             cell_update(m, s, P, g, me, F, diff, dt, pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, sh, false);
+        tile_epilogue(m, s, tile, c, part, s_red, false);
     }
 }
 
@@ -638,7 +676,7 @@ static __global__ void __launch_bounds__(256, 4) k_grad1_nodes(const DevMesh m, 
 // phs2dcns2dcellsSA (utilsFVM2dp.jl:4-17) on the current primitives and the
 // reductions that give the first step's dt (createFields2d's VMAX).
 static __global__ void __launch_bounds__(256) k_init_state(const DevMesh m, const DevState s, int64_t t0, int64_t t1) {
-    __shared__ Part sh[8];
+    __shared__ double s_red[kPartFields * 256];
     const int par = *s.parity;
     const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
     for (int64_t tile = t0 + blockIdx.x; tile < t1; tile += gridDim.x) {
@@ -658,7 +696,7 @@ static __global__ void __launch_bounds__(256) k_init_state(const DevMesh m, cons
             part.vmax = vmax;
             part.rmin = m.charlen[g] / vmax;
         }
-        tile_epilogue(m, s, tile, c, part, sh, true);
+        tile_epilogue(m, s, tile, c, part, s_red, true);
     }
 }
 
@@ -716,7 +754,7 @@ template <bool VISC, bool QUAD, bool SLOTS, int MINB>
 __global__ void __launch_bounds__(256, MINB) k_face_update(const DevMesh m, const DevState s,
                                                           double4 *__restrict__ Facc,
                                                           const double4 *__restrict__ Fslot) {
-    __shared__ Part sh[8];
+    __shared__ double s_red[kPartFields * 256];
     const int par = *s.parity;
     const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
     double4 *__restrict__ pout = s.prim + (int64_t)(par ^ 1) * m.Nc;
@@ -749,7 +787,7 @@ __global__ void __launch_bounds__(256, MINB) k_face_update(const DevMesh m, cons
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update(m, s, P, g, me, F, diff, dt, pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, sh, false);
+        tile_epilogue(m, s, tile, c, part, s_red, false);
     }
 }
 

@@ -60,6 +60,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if f.read().strip() == dig:
                 return LIB
     os.makedirs(BUILD_DIR, exist_ok=True)
+    # a failed rebuild must not leave the previous library to be loaded
+    for stale in (LIB, stamp):
+        if os.path.exists(stale):
+            os.remove(stale)
     objs, procs = [], []
     for src, extra in UNITS:  # translation units compile in parallel
         path = os.path.join(CSRC, src)
