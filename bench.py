@@ -235,7 +235,8 @@ def mixed_variant(pkg, items, s64, args, peak):
     (bit-identical to the CPU oracle in the parity tests) from the same
     initial state."""
     mesh, cfg, prims = items[0]
-    sm = pkg.solver.Solver([mesh], [cfg], pkg.solver.make_launch(precision="mixed", order=args.order, loop=args.loop))
+    sm = pkg.solver.Solver([mesh], [cfg], pkg.solver.make_launch(precision="mixed", order=args.order, loop=args.loop,
+                                                                device=args.device))
     sm.createFields2d(0, *prims)
     sm.propagate2d(args.warmup)
     sm.propagate2d(args.steps)
@@ -292,6 +293,13 @@ def main():
     args.warmup = max(args.warmup, 3, args.graph_steps if args.graph_steps > 0 else 32)
 
     world, rank, local, dist = dist_setup(args)
+    # one process per GPU: this rank's GPU (device 0 when the launcher
+    # already restricted each process to its own GPU)
+    args.device = local
+    if world > 1:
+        import torch
+        if local >= torch.cuda.device_count():
+            args.device = 0
     pkg = graft.load_package()
     items, desc, viscous = build_workload(pkg, args.config, args.precision, args.size)
     sharded = world > 1 and len(items) > 1
@@ -321,6 +329,7 @@ def main():
     meshes = [m for m, _, _ in items]
     cfgs = [c for _, c, _ in items]
     launch = pkg.solver.make_launch(precision=args.precision, order=args.order, graph_steps=args.graph_steps,
+                                    device=args.device,
                                     loop=args.loop, min_blocks=args.min_blocks, node_block=args.node_block)
     s = pkg.solver.Solver(meshes, cfgs, launch)
     for i, (_, _, p) in enumerate(items):

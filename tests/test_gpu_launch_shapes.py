@@ -80,3 +80,13 @@ def test_autotune_needs_state(pkg):
     with pytest.raises(pkg._native.NativeError):
         s.autotune(8)
     s.close()
+
+
+def test_device_out_of_range(pkg):
+    """The handle's device is named in the launch record (the library links
+    its own CUDA runtime); a device the process cannot see is an argument
+    error, not a CUDA failure."""
+    mesh, cfg, prims = pkg.cases.square_inviscid(9)
+    with pytest.raises(pkg._native.NativeError) as ei:
+        pkg.setupSolver(mesh, cfg, device=999)
+    assert "device 999" in str(ei.value)
