@@ -60,7 +60,7 @@ class Params(C.Structure):
 class Launch(C.Structure):
     _fields_ = [("precision", C.c_int32), ("order", C.c_int32), ("loop", C.c_int32), ("block", C.c_int32),
                 ("node_block", C.c_int32), ("persistent", C.c_int32), ("graph_steps", C.c_int32),
-                ("min_blocks", C.c_int32), ("stream", C.c_void_p)]
+                ("min_blocks", C.c_int32), ("device", C.c_int32), ("reserved0", C.c_int32), ("stream", C.c_void_p)]
 
 
 class Stats(C.Structure):

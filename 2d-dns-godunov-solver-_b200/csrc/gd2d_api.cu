@@ -74,6 +74,7 @@ struct gd2d_handle {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph1 = nullptr;  // one step, for the remainder of a propagate call
     int graph_steps = 0;
     bool state_ready = false;
     std::vector<std::vector<gd2d_stats>> history;
@@ -385,7 +386,26 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     h->graph_steps = h->launch.graph_steps > 0 ? h->launch.graph_steps : 32;
     h->flux = params[0].flux;
     h->visc = params[0].viscosity != GD2D_VISC_NONE;
-    cudaGetDevice(&h->device);
+    {
+        // the library links its own CUDA runtime: the caller's current
+        // device does not carry over, the launch record names the device
+        int ndev = 0;
+        cudaError_t e = cudaGetDeviceCount(&ndev);
+        if (e != cudaSuccess) {
+            delete h;
+            return fail(nullptr, GD2D_ERR_CUDA, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+        }
+        if (h->launch.device < 0 || h->launch.device >= ndev) {
+            delete h;
+            return fail(nullptr, GD2D_ERR_ARG, "device %d out of range (%d devices)", h->launch.device, ndev);
+        }
+        h->device = h->launch.device;
+        e = cudaSetDevice(h->device);
+        if (e != cudaSuccess) {
+            delete h;
+            return fail(nullptr, GD2D_ERR_CUDA, "cudaSetDevice(%d): %s", h->device, cudaGetErrorString(e));
+        }
+    }
     if (h->launch.stream) {
         h->stream = (cudaStream_t)h->launch.stream;
     } else {
@@ -898,6 +918,7 @@ static int ensure_case(gd2d_handle *h, int32_t icase) {
 
 static int drop_graph(gd2d_handle *h) {
     if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; }
+    if (h->graph1) { cudaGraphExecDestroy(h->graph1); h->graph1 = nullptr; }
     for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
     h->ev.clear();
     return GD2D_OK;
@@ -1053,6 +1074,19 @@ static int capture_graph(gd2d_handle *h, int steps, bool timing) {
     return GD2D_OK;
 }
 
+// A one-step graph (the remainder steps of a propagate call, and single-step
+// calls), timing its cell kernel with the eager event pair.
+static int capture_step_graph(gd2d_handle *h) {
+    cudaGraph_t g;
+    CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    launch_step_kernels(h, h->ev_eager[0], h->ev_eager[1], true);
+    CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&h->graph1, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    return GD2D_OK;
+}
+
 int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
     if (!h) return fail(nullptr, GD2D_ERR_ARG, "NULL handle");
     if (nsteps < 0) return fail(h, GD2D_ERR_ARG, "nsteps < 0");
@@ -1075,15 +1109,20 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
             step0[c] = h->cs_host[c].step;
             lockstep &= step0[c] == step0[0];
         }
+        // graphs this chunk needs, captured before the timed window opens
+        if (G > 1 && chunk >= G && !h->graph) {
+            int rc = capture_graph(h, G, timing);
+            if (rc) return rc;
+        }
+        if (G > 1 && chunk % G != 0 && !h->graph1) {
+            int rc = capture_step_graph(h);
+            if (rc) return rc;
+        }
         CUDA_TRY(h, cudaEventRecord(h->ev_total[0], h->stream));
         int32_t k = 0;
         bool used_graph = false;
         if (G > 1) {
             while (chunk - k >= G) {
-                if (!h->graph) {
-                    int rc = capture_graph(h, G, timing);
-                    if (rc) return rc;
-                }
                 CUDA_TRY(h, cudaGraphLaunch(h->graph, h->stream));
                 used_graph = true;
                 k += G;
@@ -1092,8 +1131,12 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
         }
         const bool time_eager = !used_graph && k < chunk;
         for (; k < chunk; ++k) {
-            const bool last = time_eager && k == chunk - 1;
-            CUDA_TRY(h, launch_step_kernels(h, last ? h->ev_eager[0] : nullptr, last ? h->ev_eager[1] : nullptr));
+            if (G > 1) {
+                CUDA_TRY(h, cudaGraphLaunch(h->graph1, h->stream));
+            } else {
+                const bool last = time_eager && k == chunk - 1;
+                CUDA_TRY(h, launch_step_kernels(h, last ? h->ev_eager[0] : nullptr, last ? h->ev_eager[1] : nullptr));
+            }
             launches += kernels_per_step(h);
         }
         CUDA_TRY(h, cudaEventRecord(h->ev_total[1], h->stream));

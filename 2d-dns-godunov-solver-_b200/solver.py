@@ -81,8 +81,9 @@ def make_params(cfg: Dict) -> N.Params:
 
 
 def make_launch(precision="f64", order="hilbert", loop="cell", block=0, node_block=0, persistent=0,
-                graph_steps=0, stream=None, min_blocks=0) -> N.Launch:
+                graph_steps=0, stream=None, min_blocks=0, device=0) -> N.Launch:
     l = N.Launch()
+    l.device = int(device)
     l.precision = N.PRECISION[precision] if isinstance(precision, str) else int(precision)
     l.order = N.ORDER[order] if isinstance(order, str) else int(order)
     l.loop = N.LOOP[loop] if isinstance(loop, str) else int(loop)

@@ -131,8 +131,11 @@ typedef struct gd2d_launch {
     int32_t node_block;     /* threads per block of the node kernel (0 = default) */
     int32_t persistent;     /* 1: grid-stride persistent cell kernel */
     int32_t graph_steps;    /* steps per captured CUDA graph (0 = default, 1 = eager) */
-    int32_t min_blocks;     /* cell kernel blocks per SM the register budget targets: 2, 3 (default), 4 */
-    void *stream;           /* cudaStream_t to run on; NULL: the handle's own */
+    int32_t min_blocks;     /* cell kernel blocks per SM the register budget targets: 2, 3, 4 (0 = default) */
+    int32_t device;         /* CUDA device ordinal of the handle (the library links its own CUDA
+                               runtime, so the caller's current device does not carry over) */
+    int32_t reserved0;
+    void *stream;           /* cudaStream_t to run on (on `device`); NULL: the handle's own */
 } gd2d_launch;
 
 /* Per-case diagnostics of one step (the reference's dynControls fields,
