@@ -189,9 +189,9 @@ def cpu_model() -> str:
 
 def cpu_reference(pkg, items, steps, warmup, budget_s=25.0, single_thread_s=8.0):
     """Time the CPU restatement of the reference step (oracle) on a bounded
-    sample of the workload: all host threads, one warm-up step, then five
-    timed repeats of equal length (median reported); plus a one-thread
-    figure on a step or two."""
+    sample of the workload: all host threads, `warmup` untimed steps (at
+    least 3, at most ~10 s of them), then five timed repeats of equal length
+    (median reported); plus a one-thread figure on a step or two."""
     from oracle import oracle as orc
     orc.build()
     nthreads = os.cpu_count() or 1
@@ -202,6 +202,9 @@ def cpu_reference(pkg, items, steps, warmup, budget_s=25.0, single_thread_s=8.0)
     t0 = time.perf_counter()
     o.step()
     t1 = time.perf_counter() - t0
+    n_warm = max(3, min(warmup, int(10.0 / max(t1, 1e-6))))
+    for _ in range(n_warm - 1):
+        o.step()
     reps = 5
     per_rep = max(1, min(steps, int(budget_s / reps / max(t1, 1e-6))))
     rates = []
@@ -224,8 +227,8 @@ def cpu_reference(pkg, items, steps, warmup, budget_s=25.0, single_thread_s=8.0)
             o1.step()
         single = cells * n1 / (time.perf_counter() - t0) / 1e6
     return {"value": rates[len(rates) // 2], "unit": "Mcell-steps/s", "cores": nthreads, "kind": "port",
-            "sample": f"median of {reps} repeats of {per_rep} steps of case 0 ({cells} cells) after 1 warm-up "
-                      f"step, {nthreads} threads",
+            "sample": f"median of {reps} repeats of {per_rep} steps of case 0 ({cells} cells) after {n_warm} "
+                      f"warm-up steps, {nthreads} threads", "warmup": n_warm,
             "repeats": [round(r, 4) for r in rates], "single_thread_value": single, "host": cpu_model()}
 
 
@@ -238,7 +241,7 @@ def mixed_variant(pkg, items, s64, args, peak):
     sm = pkg.solver.Solver([mesh], [cfg], pkg.solver.make_launch(precision="mixed", order=args.order, loop=args.loop,
                                                                 device=args.device))
     sm.createFields2d(0, *prims)
-    sm.propagate2d(args.warmup)
+    sm.propagate2d(args.gpu_warmup)
     sm.propagate2d(args.steps)
     tot, cell_ms, _ = sm.last_timing()
     value = mesh.nCells * args.steps / (tot / 1e3) / 1e6
@@ -290,7 +293,10 @@ def main():
                     help="steps of the mixed-vs-FP64 error measurement")
     args = ap.parse_args()
     # at least 3 warm-up steps, and at least one CUDA graph's worth
-    args.warmup = max(args.warmup, 3, args.graph_steps if args.graph_steps > 0 else 32)
+    args.warmup = max(args.warmup, 3)
+    # the GPU arm warms up at least one CUDA graph's worth of steps
+    gpu_warmup = max(args.warmup, args.graph_steps if args.graph_steps > 0 else 32)
+    args.gpu_warmup = gpu_warmup
 
     world, rank, local, dist = dist_setup(args)
     # one process per GPU: this rank's GPU (device 0 when the launcher
@@ -317,7 +323,7 @@ def main():
             return
         cb = cpu_reference(pkg, items, args.steps, args.warmup, budget_s=60.0)
         line = {"impl": "reference", "metric": metric, "value": cb["value"], "unit": cb["unit"], "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "steps": args.steps, "warmup": cb["warmup"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg_line,
                 "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "repeats",
                                                     "single_thread_value", "host")},
@@ -342,7 +348,7 @@ def main():
     # captured and instantiated before the timed region; the clock sampler
     # starts first, its start-up away from the timed region
     with ClockSampler(local) as clk:
-        s.propagate2d(args.warmup)
+        s.propagate2d(gpu_warmup)
         dist_barrier(dist)
         s.propagate2d(args.steps)
         total_ms, cell_ms, launches = s.last_timing()
@@ -384,7 +390,7 @@ def main():
     traffic = tpc * cells if tpc else None
     traffic_src = ("ncu dram bytes per cell of one launch x cells (%.0f B/cell)" % tpc) if tpc else None
     line = {"metric": metric, "value": value, "unit": "Mcell-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": gpu_warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "f64" else "f32+f64",
             "data": "synthetic (seeded generated meshes and initial states)", "config": cfg_line,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
