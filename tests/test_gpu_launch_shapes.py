@@ -40,15 +40,15 @@ def test_launch_shape_is_bit_exact(pkg, shape):
     assert [h["dt"] for h in href] == [h["dt"] for h in hgot]
 
 
-@pytest.mark.parametrize("precision", ["f64", "mixed"])
-def test_autotune_restores_state(pkg, precision):
+@pytest.mark.parametrize("precision,loop", [("f64", "cell"), ("f64", "tile"), ("mixed", "cell"), ("mixed", "tile")])
+def test_autotune_restores_state(pkg, precision, loop):
     """The trials leave no trace: the state right after gd2d_autotune is the
     state before it, and the run continues from there (FP64: bit-identical
     to a run that never tuned; mixed: its FP32 arithmetic may round
     differently under another register budget, so within 1e-6)."""
     mesh, cfg, prims = _viscous_case(pkg)
-    ref, href = _run(pkg, mesh, cfg, prims, 30, precision=precision)
-    s = pkg.setupSolver(mesh, cfg, precision=precision)
+    ref, href = _run(pkg, mesh, cfg, prims, 30, precision=precision, loop=loop)
+    s = pkg.setupSolver(mesh, cfg, precision=precision, loop=loop)
     s.createFields2d(0, *prims)
     s.propagate2d(10)
     before = s.get_state(0)
