@@ -31,12 +31,11 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
     for (int64_t tile = blockIdx.x; tile < m.ntiles; tile += gridDim.x) {
         const int c = m.tile_case[tile];
         const DevCase &P = m.cases[c];
-        const double dt = s.cstate[c].dt, t = s.cstate[c].t;
+        const double t = s.cstate[c].t;
         const int64_t base = tile * B;
         const int64_t g = base + threadIdx.x;
         const bool venkat = P.limiter == LIM_VENKAT;
-        const float4 me = pin[g];
-        s_prim[threadIdx.x] = me;
+        s_prim[threadIdx.x] = pin[g];
         if (venkat) s_hx[threadIdx.x] = m.hxf[g];
         __syncthreads();
         const float gam = (float)P.gamma;
@@ -74,6 +73,10 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
             if (tf.lbp) s_flux[tf.kb][tf.lbp - 1] = make_float4(-fv[0], -fv[1], -fv[2], -fv[3]);
         }
         // the viscous source needs no flux: evaluated before the barrier
+        // (the cell's primitives re-read from the stage, not held through
+        // the face phase)
+        const float4 me = s_prim[threadIdx.x];
+        const double dt = s.cstate[c].dt;
         const int4 nb = m.nbr[g];
         const bool is_quad = QUAD && (nb.w != kAbsent);
         float diff[4] = {0.f, 0.f, 0.f, 0.f};

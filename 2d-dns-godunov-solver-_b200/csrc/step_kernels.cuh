@@ -459,12 +459,11 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
     for (int64_t tile = blockIdx.x; tile < m.ntiles; tile += gridDim.x) {
         const int c = m.tile_case[tile];
         const DevCase &P = m.cases[c];
-        const double dt = s.cstate[c].dt, t = s.cstate[c].t;
+        const double t = s.cstate[c].t;
         const int64_t base = tile * B;
         const int64_t g = base + threadIdx.x;
         const bool venkat = P.limiter == LIM_VENKAT;
-        const double4 me = pin[g];
-        s_prim[threadIdx.x] = me;
+        s_prim[threadIdx.x] = pin[g];
         if (venkat) s_hx[threadIdx.x] = m.hx[g];
         __syncthreads();
         const double gam = P.gamma;
@@ -499,6 +498,10 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
         }
         // the cell's viscous source needs no flux: evaluated before the
         // barrier, it fills the time a thread with fewer faces would wait
+        // (the cell's primitives are re-read from the stage rather than
+        // held in registers through the face phase)
+        const double4 me = s_prim[threadIdx.x];
+        const double dt = s.cstate[c].dt;
         const int4 nb = m.nbr[g];
         const bool is_quad = QUAD && (nb.w != kAbsent);
         double diff[4] = {0.0, 0.0, 0.0, 0.0};
