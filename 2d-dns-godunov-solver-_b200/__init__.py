@@ -9,7 +9,7 @@ of the reference's setupSolver/propagate2d call shape.
 """
 from . import mesh, cases, solver  # noqa: F401
 from .mesh import Mesh2d  # noqa: F401
-from .solver import Solver, setupSolver  # noqa: F401
+from .solver import Solver, propagate_until_converged, setupSolver, updateResidualSA  # noqa: F401
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

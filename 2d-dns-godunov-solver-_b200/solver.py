@@ -241,6 +241,44 @@ class Solver:
         return D
 
 
+def updateResidualSA(history: Sequence[Dict], convergence_criteria: Sequence[float]) -> Tuple[List[float], int]:
+    """The reference's residual bookkeeping (updateResidualSA,
+    evaluate2d.jl:1-41) over a case's step history, step 1 first.
+
+    residualsVectorMax starts at ones and is the running max of the first
+    curIter residuals while 1 < curIter < 6 (curIter = the 1-based step);
+    the solution is converged at the first curIter > 5 where every
+    residual divided by its max is <= its criterion.  Returns
+    (residualsVectorMax, converged step or 0)."""
+    rmax = [1.0, 1.0, 1.0, 1.0]
+    crit = [float(c) for c in convergence_criteria]
+    for it in range(1, len(history) + 1):
+        if 1 < it < 6:
+            rmax = [max(h["residual"][v] for h in history[:it]) for v in range(4)]
+        if it > 5 and all(history[it - 1]["residual"][v] / rmax[v] <= crit[v] for v in range(4)):
+            return rmax, it
+    return rmax, 0
+
+
+def propagate_until_converged(solver: "Solver", icase: int, max_steps: int, convergence_criteria: Sequence[float],
+                              chunk: int = 256) -> int:
+    """The reference's run loop (testInviscidFluxesGPUx32.jl:314-447): step
+    until the residual criterion of updateResidualSA holds or max_steps
+    steps have run, in chunks of `chunk` steps (one CUDA graph replay per
+    32 steps; the convergence test runs on the host between chunks, so up
+    to chunk-1 steps past convergence may run).  Returns the converged step
+    (1-based, since the case's state was set) or 0."""
+    done = 0
+    while done < max_steps:
+        n = min(chunk, max_steps - done)
+        solver.propagate2d(n)
+        done += n
+        _, conv = updateResidualSA(solver.history(icase), convergence_criteria)
+        if conv:
+            return conv
+    return 0
+
+
 def setupSolver(meshes, cfgs, **launch_kw) -> Solver:
     """setupSolver_*.jl + device setup for one or more cases."""
     if isinstance(meshes, Mesh2d):

@@ -324,3 +324,19 @@ def test_tiny_and_ragged_meshes(pkg, orc, loop, which):
     else:
         assert np.array_equal(g["Ucons"], o.field("Uold"))
         assert np.array_equal(g["node_prims"], o.node_prims())
+
+
+def test_propagate_until_converged_matches_history(pkg):
+    """The reference's run loop: stepping in chunks until updateResidualSA's
+    criterion holds stops at the step the full history says (checked
+    between chunks, so within one chunk of it)."""
+    mesh, cfg, prims = pkg.cases.square_inviscid(21)
+    s = pkg.setupSolver(mesh, cfg)
+    s.createFields2d(0, *prims)
+    crit = [1e-2] * 4
+    conv = pkg.propagate_until_converged(s, 0, 2000, crit, chunk=64)
+    h = s.history(0)
+    s.close()
+    _, first = pkg.updateResidualSA(h, crit)
+    assert conv == first and conv > 5
+    assert len(h) - 64 < conv <= len(h)

@@ -138,3 +138,19 @@ def test_reference_mesh_face_mirrors(pkg):
     tot, good = _face_pair_symmetry(m)
     print("reference mesh: %d of %d interior faces are exact mirrors" % (good, tot))
     assert tot > 0
+
+
+def test_update_residual_bookkeeping(pkg):
+    """updateResidualSA (evaluate2d.jl:1-41): the running max over steps
+    2-5 normalises the residuals; convergence is the first step > 5 where
+    every normalised residual is within its criterion."""
+    def hist(vals):
+        return [{"residual": [v, 2 * v, 3 * v, 4 * v]} for v in vals]
+    h = hist([1.0, 8.0, 4.0, 2.0, 1.0, 0.5, 0.1, 0.004, 0.001])
+    rmax, conv = pkg.updateResidualSA(h, [1e-3] * 4)
+    assert rmax == [8.0, 16.0, 24.0, 32.0]
+    assert conv == 8          # 0.004 / 8 <= 1e-3 first at step 8 (0.1 / 8 > 1e-3 at step 7)
+    rmax, conv = pkg.updateResidualSA(h, [0.05] * 4)
+    assert conv == 7          # 0.1 / 8 <= 0.05 at step 7 (step 6: 0.5 / 8 > 0.05)
+    assert pkg.updateResidualSA(h[:3], [1.0] * 4) == ([8.0, 16.0, 24.0, 32.0], 0)
+    assert pkg.updateResidualSA([], [1.0] * 4) == ([1.0, 1.0, 1.0, 1.0], 0)
