@@ -12,9 +12,10 @@ time step over all cells.  Synthetic, seeded inputs (no dataset exists).
 value: cell-steps/s (Mcell-steps/s) with state resident in HBM, device
 time from CUDA events on the solver's stream, max over ranks.  The working
 set (~0.9 GB) is far larger than L2, so no flush is needed between steps.
-e2e: the same metric through the C ABI with host buffers: set_state from
-pinned host memory, K x gd2d_propagate(h, 1, stats) (per-step stats read
-back), gd2d_get_state of the final state.
+e2e: the same metric through the C ABI with host buffers: set_state of
+every case from host arrays (through the library's page-locked stage),
+K x gd2d_propagate(h, 1, stats) (per-step stats read back), gd2d_get_state
+of every case's final conservatives.
 """
 from __future__ import annotations
 
@@ -360,27 +361,30 @@ def main():
     value = job_cells * args.steps / (total_ms / 1e3) / 1e6
     ms_per_step = total_ms / args.steps
 
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers: every case's state
+    # uploaded from the host, K single-step calls with the statistics read
+    # back each step, every case's conservatives read back at the end
     import ctypes as C
     N = pkg._native
     L = N.load()
-    m0 = meshes[0]
-    host_prims = [np.ascontiguousarray(x, dtype=np.float64) for x in items[0][2]]
-    ucons = np.zeros((m0.nCells, 4), order="F")
+    host_prims = [[np.ascontiguousarray(x, dtype=np.float64) for x in it[2]] for it in items]
+    ucons = [np.zeros((m.nCells, 4), order="F") for m in meshes]
     st = (N.Stats * len(meshes))()
     dp = C.POINTER(C.c_double)
     dist_barrier(dist)
     e2e_steps = args.steps
     t0 = time.perf_counter()
-    N.check(L.gd2d_set_state(s.h, 0, *[a.ctypes.data_as(dp) for a in host_prims]), s.h)
+    for i, hp in enumerate(host_prims):
+        N.check(L.gd2d_set_state(s.h, i, *[a.ctypes.data_as(dp) for a in hp]), s.h)
     for _ in range(e2e_steps):
         N.check(L.gd2d_propagate(s.h, 1, st), s.h)
-    N.check(L.gd2d_get_state(s.h, 0, ucons.ctypes.data_as(dp), None, None), s.h)
+    for i, u in enumerate(ucons):
+        N.check(L.gd2d_get_state(s.h, i, u.ctypes.data_as(dp), None, None), s.h)
     e2e_s = time.perf_counter() - t0
     e2e_s = dist_max(dist, e2e_s)
-    e2e_val = m0.nCells * e2e_steps * world / e2e_s / 1e6
-    h2d = 4 * 8 * m0.nCells / e2e_steps
-    d2h = C.sizeof(N.Stats) * len(meshes) + 4 * 8 * m0.nCells / e2e_steps
+    e2e_val = job_cells * e2e_steps / e2e_s / 1e6
+    h2d = 4 * 8 * cells / e2e_steps
+    d2h = C.sizeof(N.Stats) * len(meshes) + 4 * 8 * cells / e2e_steps
 
     peak, peak_kind = load_peaks()
     alg = ALG_BYTES[(args.precision, viscous)]
