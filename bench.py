@@ -286,6 +286,8 @@ def main():
     ap.add_argument("--min-blocks", type=int, default=0, help="cell-kernel register budget (0: library default)")
     ap.add_argument("--node-block", type=int, default=0)
     ap.add_argument("--size", type=int, default=1025, help="cylinder: nodes per side")
+    ap.add_argument("--flux", default=None, choices=["ausm", "roe", "ausm_m2020"],
+                    help="override the workload's face flux (cylinder: AUSM+)")
     ap.add_argument("--autotune", action="store_true",
                     help="let gd2d_autotune pick the launch shape before the warm-up")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -309,6 +311,9 @@ def main():
             args.device = 0
     pkg = graft.load_package()
     items, desc, viscous = build_workload(pkg, args.config, args.precision, args.size)
+    if args.flux:
+        items = [(m, dict(c, flux=args.flux), p) for m, c, p in items]
+        desc = dict(desc, flux=args.flux)
     sharded = world > 1 and len(items) > 1
     if sharded:
         # independent cases split across ranks (no data exchange), balanced by cells
@@ -407,7 +412,7 @@ def main():
                          "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak},
             "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "clocks": clocks}
-    if args.config == "cylinder" and args.precision == "f64" and not args.no_mixed:
+    if args.config in ("cylinder", "square") and args.precision == "f64" and not args.no_mixed:
         line["mixed"] = mixed_variant(pkg, items, s, args, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(pkg, items, args.steps, args.warmup)
