@@ -246,7 +246,7 @@ def mixed_variant(pkg, items, s64, args, peak):
     sm.propagate2d(args.steps)
     tot, cell_ms, _ = sm.last_timing()
     value = mesh.nCells * args.steps / (tot / 1e3) / 1e6
-    alg = ALG_BYTES[("mixed", True)]
+    alg = ALG_BYTES[("mixed", cfg.get("viscosity", "none") != "none")]
     # error run: both paths from the initial state
     n_err = args.error_steps
     sm.createFields2d(0, *prims)
