@@ -16,6 +16,22 @@
 
 namespace gd2d {
 
+// Loads and stores of data a step touches once (per-cell and per-face mesh
+// arrays, the conservative state): marked evict-first, so that the caches
+// keep the gathered node and neighbour data instead.
+template <class T>
+__device__ __forceinline__ T ld_once(const T *p) {
+    return __ldcs(p);
+}
+__device__ __forceinline__ double4 ld_once(const double4 *p) {
+    const double2 a = __ldcs(reinterpret_cast<const double2 *>(p)), b = __ldcs(reinterpret_cast<const double2 *>(p) + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void st_once(double4 *p, const double4 &v) {
+    __stcs(reinterpret_cast<double2 *>(p), make_double2(v.x, v.y));
+    __stcs(reinterpret_cast<double2 *>(p) + 1, make_double2(v.z, v.w));
+}
+
 __device__ __forceinline__ int nbr_k(const int4 &v, int k) {
     return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
 }
@@ -290,8 +306,8 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
     const bool art = (P.visc_model != VISC_REFERENCE) && P.art_visc;
     for (int k = 0; k < nf; ++k) {
         const int64_t o = (int64_t)k * m.Nc + g;
-        const double side = m.len[o], nx = m.nx[o], ny = m.ny[o];
-        const int2 e = m.c2n[o];
+        const double side = ld_once(m.len + o), nx = ld_once(m.nx + o), ny = ld_once(m.ny + o);
+        const int2 e = ld_once(m.c2n + o);
         const NodeGrad A = s.nodeG[e.x], B = s.nodeG[e.y];
         double fx, fy;
         fx = 0.5 * (A.ru.x + B.ru.x) * -ny * side; fy = 0.5 * (A.ru.y + B.ru.y) * -nx * side;
@@ -308,7 +324,7 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
             dv = (k == 0) ? fv : dv + fv;
         }
     }
-    const double area = m.area[g];
+    const double area = ld_once(m.area + g);
     double lap[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) lap[v] = sx[v] / area + sy[v] / area;
@@ -323,7 +339,7 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
         const double mu = (P.visc_model == VISC_SUTHERLAND) ? P.mu_ref * (sutherland(T) / P.suth_ref) : P.mu_ref;
         double mart = 0.0;
         if (art) {
-            const double HX = m.hx[g];
+            const double HX = ld_once(m.hx + g);
             const double divU = du / area + dv / area;
             const double aS = sqrt(P.gamma * me.w / me.x);
             const double a = 0.05 * aS / HX / sqrt(2.0);
@@ -346,8 +362,8 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
 __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
                                             const double4 &me, const double *F, const double *diff, double dt,
                                             double4 *__restrict__ pout, Part &part) {
-    const double rarea = m.rarea[g];
-    const double4 U = s.U[g];
+    const double rarea = ld_once(m.rarea + g);
+    const double4 U = ld_once(s.U + g);
     const double Uo[4] = {U.x, U.y, U.z, U.w};
     double Un[4];
 #pragma unroll
@@ -356,7 +372,7 @@ __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s,
         if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
         if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
     }
-    s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
+    st_once(s.U + g, make_double4(Un[0], Un[1], Un[2], Un[3]));
     const double gam = P.gamma;
     const double rho = Un[0];
     const double ux = Un[1] / Un[0];
@@ -365,7 +381,7 @@ __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s,
     const double a = sqrt(gam * p / rho);
     const double vmax = sqrt(ux * ux + uy * uy) + a;
     pout[g] = make_double4(rho, ux, uy, p);
-    const double area = m.area[g];
+    const double area = ld_once(m.area + g);
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
         const double d = Un[v] - Uo[v];
@@ -374,7 +390,7 @@ __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s,
     }
     part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
     part.vmax = vmax;
-    part.rmin = m.charlen[g] / vmax;
+    part.rmin = ld_once(m.charlen + g) / vmax;
     part.rhomin = me.x;
     part.rhomax = me.x;
     const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
@@ -464,13 +480,13 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
         const int64_t g = base + threadIdx.x;
         const bool venkat = P.limiter == LIM_VENKAT;
         s_prim[threadIdx.x] = pin[g];
-        if (venkat) s_hx[threadIdx.x] = m.hx[g];
+        if (venkat) s_hx[threadIdx.x] = ld_once(m.hx + g);
         __syncthreads();
         const double gam = P.gamma;
         const double g2 = 2.0 * (gam - 1.0) / (gam + 1.0);
         const int64_t f1 = m.tf_off[tile + 1];
         for (int64_t f = m.tf_off[tile] + threadIdx.x; f < f1; f += B) {
-            const int4 rec = m.tf_rec[f];
+            const int4 rec = ld_once(m.tf_rec + f);
             const TileFace tf = unpack_tile_face(rec.y);
             const double4 a4 = s_prim[tf.la];
             const double uL[4] = {a4.x, a4.y, a4.z, a4.w};
@@ -491,7 +507,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
             if (QUAD && tf.quad) q2 = m.tf_q[f];
             double fv[4];
             face_flux_at<FLUX, QUAD>(m, P, s.nodeP, base + tf.la, tf.ka, rec.x, rec.z, rec.w, q2.x, q2.y,
-                                     QUAD && tf.quad, uL, r, hx_own, hxR, m.tf_len[f], m.tf_nx[f], m.tf_ny[f], t,
+                                     QUAD && tf.quad, uL, r, hx_own, hxR, ld_once(m.tf_len + f), ld_once(m.tf_nx + f), ld_once(m.tf_ny + f), t,
                                      g2, fv);
             s_flux[tf.ka][tf.la] = make_double4(fv[0], fv[1], fv[2], fv[3]);
             if (tf.lbp) s_flux[tf.kb][tf.lbp - 1] = make_double4(-fv[0], -fv[1], -fv[2], -fv[3]);
@@ -502,7 +518,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
         // held in registers through the face phase)
         const double4 me = s_prim[threadIdx.x];
         const double dt = s.cstate[c].dt;
-        const int4 nb = m.nbr[g];
+        const int4 nb = ld_once(m.nbr + g);
         const bool is_quad = QUAD && (nb.w != kAbsent);
         double diff[4] = {0.0, 0.0, 0.0, 0.0};
         if (VISC && nb.x != kAbsent) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);

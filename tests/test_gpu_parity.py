@@ -329,14 +329,22 @@ def test_tiny_and_ragged_meshes(pkg, orc, loop, which):
 def test_propagate_until_converged_matches_history(pkg):
     """The reference's run loop: stepping in chunks until updateResidualSA's
     criterion holds stops at the step the full history says (checked
-    between chunks, so within one chunk of it)."""
+    between chunks, so within one chunk of it).  The criterion is the
+    normalised residual a first run reaches at step 150."""
     mesh, cfg, prims = pkg.cases.square_inviscid(21)
+    a = pkg.setupSolver(mesh, cfg)
+    a.createFields2d(0, *prims)
+    a.propagate2d(300)
+    ha = a.history(0)
+    a.close()
+    rmax, _ = pkg.updateResidualSA(ha, [0.0] * 4)
+    crit = [ha[149]["residual"][v] / rmax[v] * (1 + 1e-12) for v in range(4)]
     s = pkg.setupSolver(mesh, cfg)
     s.createFields2d(0, *prims)
-    crit = [1e-2] * 4
-    conv = pkg.propagate_until_converged(s, 0, 2000, crit, chunk=64)
+    conv = pkg.propagate_until_converged(s, 0, 300, crit, chunk=64)
     h = s.history(0)
     s.close()
     _, first = pkg.updateResidualSA(h, crit)
-    assert conv == first and conv > 5
+    assert 5 < conv <= 150 and conv == first
     assert len(h) - 64 < conv <= len(h)
+
