@@ -36,13 +36,13 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
         const int64_t g = base + threadIdx.x;
         const bool venkat = P.limiter == LIM_VENKAT;
         s_prim[threadIdx.x] = pin[g];
-        if (venkat) s_hx[threadIdx.x] = m.hxf[g];
+        if (venkat) s_hx[threadIdx.x] = ld_once(m.hxf + g);
         __syncthreads();
         const float gam = (float)P.gamma;
         const float g2 = 2.f * (gam - 1.f) / (gam + 1.f);
         const int64_t f1 = m.tf_off[tile + 1];
         for (int64_t f = m.tf_off[tile] + threadIdx.x; f < f1; f += B) {
-            const int4 rec = m.tf_rec[f];
+            const int4 rec = ld_once(m.tf_rec + f);
             const TileFace tf = unpack_tile_face(rec.y);
             const float4 a4 = s_prim[tf.la];
             const float uL[4] = {a4.x, a4.y, a4.z, a4.w};
@@ -67,7 +67,8 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
                 }
             }
             float fv[4];
-            face_flux_pre<FLUX>(m, P, base + tf.la, tf.ka, rec.x, r, dd, uu, m.tf_nxf[f], m.tf_nyf[f], m.tf_lenf[f],
+            face_flux_pre<FLUX>(m, P, base + tf.la, tf.ka, rec.x, r, dd, uu, ld_once(m.tf_nxf + f), ld_once(m.tf_nyf + f),
+                                ld_once(m.tf_lenf + f),
                                 uL, hx_own, hxR, t, g2, fv);
             s_flux[tf.ka][tf.la] = make_float4(fv[0], fv[1], fv[2], fv[3]);
             if (tf.lbp) s_flux[tf.kb][tf.lbp - 1] = make_float4(-fv[0], -fv[1], -fv[2], -fv[3]);
@@ -77,7 +78,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
         // the face phase)
         const float4 me = s_prim[threadIdx.x];
         const double dt = s.cstate[c].dt;
-        const int4 nb = m.nbr[g];
+        const int4 nb = ld_once(m.nbr + g);
         const bool is_quad = QUAD && (nb.w != kAbsent);
         float diff[4] = {0.f, 0.f, 0.f, 0.f};
         if (VISC && nb.x != kAbsent) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);

@@ -116,8 +116,8 @@ __device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &
     const bool art = (P.visc_model != VISC_REFERENCE) && P.art_visc;
     for (int k = 0; k < nf; ++k) {
         const int64_t o = (int64_t)k * m.Nc + g;
-        const float side = m.lenf[o], nx = m.nxf[o], ny = m.nyf[o];
-        const int2 e = m.c2n[o];
+        const float side = ld_once(m.lenf + o), nx = ld_once(m.nxf + o), ny = ld_once(m.nyf + o);
+        const int2 e = ld_once(m.c2n + o);
         const NodeGradF A = s.nodeGf[e.x], B = s.nodeGf[e.y];
         sx[0] += 0.5f * (A.ru.x + B.ru.x) * -ny * side; sy[0] += 0.5f * (A.ru.y + B.ru.y) * -nx * side;
         sx[1] += 0.5f * (A.rv.x + B.rv.x) * -ny * side; sy[1] += 0.5f * (A.rv.y + B.rv.y) * -nx * side;
@@ -128,7 +128,7 @@ __device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &
             dv += 0.5f * (na.z + nb.z) * -ny * side;
         }
     }
-    const float rA = m.rareaf[g];
+    const float rA = ld_once(m.rareaf + g);
     float lap[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) lap[v] = (sx[v] + sy[v]) * rA;
@@ -145,7 +145,7 @@ __device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &
                              : (float)P.mu_ref;
         float mart = 0.f;
         if (art) {
-            const float HX = m.hxf[g];
+            const float HX = ld_once(m.hxf + g);
             const float divU = (du + dv) * rA;
             const float aS = sqrtf((float)P.gamma * me.w / me.x);
             const float a = 0.05f * aS / HX * 0.70710678f;
@@ -169,8 +169,8 @@ __device__ __forceinline__ void cell_update_mixed(const DevMesh &m, const DevSta
                                                   const float4 &me, const float *F, const float *diff, double dt,
                                                   float4 *__restrict__ pout, Part &part) {
     const float bdt = (float)(P.beta * dt);
-    const float rarea = m.rareaf[g];
-    const double4 U = s.U[g];
+    const float rarea = ld_once(m.rareaf + g);
+    const double4 U = ld_once(s.U + g);
     const double Uo[4] = {U.x, U.y, U.z, U.w};
     double Un[4];
 #pragma unroll
@@ -179,7 +179,7 @@ __device__ __forceinline__ void cell_update_mixed(const DevMesh &m, const DevSta
         if (Un[0] >= P.rho_max) Un[0] = P.rho_max;
         if (Un[0] <= P.rho_min) Un[0] = P.rho_min;
     }
-    s.U[g] = make_double4(Un[0], Un[1], Un[2], Un[3]);
+    st_once(s.U + g, make_double4(Un[0], Un[1], Un[2], Un[3]));
     const double rho = Un[0];
     const double rinv = 1.0 / rho;
     const double ux = Un[1] * rinv;
@@ -188,7 +188,7 @@ __device__ __forceinline__ void cell_update_mixed(const DevMesh &m, const DevSta
     const float a = sqrtf((float)(P.gamma * p * rinv));
     const float vmax = sqrtf((float)(ux * ux + uy * uy)) + a;
     pout[g] = make_float4((float)rho, (float)ux, (float)uy, (float)p);
-    const double area = (double)m.areaf[g];
+    const double area = (double)ld_once(m.areaf + g);
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
         const double d = Un[v] - Uo[v];
@@ -197,7 +197,7 @@ __device__ __forceinline__ void cell_update_mixed(const DevMesh &m, const DevSta
     }
     part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
     part.vmax = (double)vmax;
-    part.rmin = (double)(m.charlenf[g] / vmax);
+    part.rmin = (double)(ld_once(m.charlenf + g) / vmax);
     part.rhomin = (double)me.x;
     part.rhomax = (double)me.x;
     const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
