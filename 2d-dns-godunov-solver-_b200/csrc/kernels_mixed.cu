@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(256, 6) k_node_avg_mixed(const DevMesh m, cons
         bool prim_form = false;
         float gop = 0.f, gam = 0.f;
         if (VISC) {
-            const DevCase &P = m.cases[m.node_case[J]];
+            const DevCase &P = m.cases[ld_once(m.node_case + J)];
             prim_form = P.visc_model != VISC_REFERENCE;
             gop = (float)P.gamma_over_Pr;
             gam = (float)P.gamma;
@@ -112,13 +112,13 @@ __global__ void __launch_bounds__(256, 6) k_node_avg_mixed(const DevMesh m, cons
         };
         int ci[kMaxCluster];
 #pragma unroll
-        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? m.cl[(int64_t)j * m.Nn + J] : -1;
+        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? ld_once(m.cl + (int64_t)j * m.Nn + J) : -1;
 #pragma unroll
         for (int j = 0; j < kMaxCluster; ++j)
-            if (ci[j] >= 0) add(ci[j], src[ci[j]], UNIT ? 1.f : (float)m.wt[(int64_t)j * m.Nn + J]);
+            if (ci[j] >= 0) add(ci[j], src[ci[j]], UNIT ? 1.f : (float)ld_once(m.wt + (int64_t)j * m.Nn + J));
         for (int j = kMaxCluster; j < W; ++j) {
-            const int c = m.cl[(int64_t)j * m.Nn + J];
-            if (c >= 0) add(c, src[c], UNIT ? 1.f : (float)m.wt[(int64_t)j * m.Nn + J]);
+            const int c = ld_once(m.cl + (int64_t)j * m.Nn + J);
+            if (c >= 0) add(c, src[c], UNIT ? 1.f : (float)ld_once(m.wt + (int64_t)j * m.Nn + J));
         }
         if (det != 0.f) { const float r = 1.f / det; a0 *= r; a1 *= r; a2 *= r; a3 *= r; }
         s.nodePf[J] = zero_prims ? make_float4(0.f, 0.f, 0.f, 0.f) : make_float4(a0, a1, a2, a3);
@@ -147,19 +147,19 @@ template <bool QUAD>
 __global__ void __launch_bounds__(256, 6) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         // padding cells have zero area; triangles a zero-length fourth edge
-        if (m.areaf[g] == 0.f) continue;
-        const int nf = (QUAD && m.lenf[3 * m.Nc + g] != 0.f) ? 4 : 3;
+        if (ld_once(m.areaf + g) == 0.f) continue;
+        const int nf = (QUAD && ld_once(m.lenf + 3 * m.Nc + g) != 0.f) ? 4 : 3;
         float sx[3] = {0.f, 0.f, 0.f}, sy[3] = {0.f, 0.f, 0.f};
         for (int k = 0; k < nf; ++k) {
             const int64_t o = (int64_t)k * m.Nc + g;
-            const float side = m.lenf[o], nx = m.nxf[o], ny = m.nyf[o];
-            const int2 e = m.c2n[o];
+            const float side = ld_once(m.lenf + o), nx = ld_once(m.nxf + o), ny = ld_once(m.nyf + o);
+            const int2 e = ld_once(m.c2n + o);
             const float4 A = s.nodeCf[e.x], B = s.nodeCf[e.y];
             sx[0] += 0.5f * (A.x + B.x) * -ny * side; sy[0] += 0.5f * (A.x + B.x) * -nx * side;
             sx[1] += 0.5f * (A.y + B.y) * -ny * side; sy[1] += 0.5f * (A.y + B.y) * -nx * side;
             sx[2] += 0.5f * (A.z + B.z) * -ny * side; sy[2] += 0.5f * (A.z + B.z) * -nx * side;
         }
-        const float rA = m.rareaf[g];
+        const float rA = ld_once(m.rareaf + g);
         NodeGradF r;
         r.ru = make_float2(sx[0] * rA, sy[0] * rA);
         r.rv = make_float2(sx[1] * rA, sy[1] * rA);
@@ -179,12 +179,12 @@ __global__ void __launch_bounds__(256, 6) k_grad1_nodes_mixed(const DevMesh m, c
         };
         int ci[kMaxCluster];
 #pragma unroll
-        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? m.cl[(int64_t)j * m.Nn + J] : -1;
+        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? ld_once(m.cl + (int64_t)j * m.Nn + J) : -1;
 #pragma unroll
         for (int j = 0; j < kMaxCluster; ++j)
             if (ci[j] >= 0) add(s.g1f[ci[j]]);
         for (int j = kMaxCluster; j < W; ++j) {
-            const int c = m.cl[(int64_t)j * m.Nn + J];
+            const int c = ld_once(m.cl + (int64_t)j * m.Nn + J);
             if (c >= 0) add(s.g1f[c]);
         }
         const float r = cnt ? 1.f / (float)cnt : 0.f;

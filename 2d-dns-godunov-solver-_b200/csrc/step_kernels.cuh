@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(256, 4) k_node_avg(const DevMesh m, const DevS
         bool prim_form = false;
         double gop = 0.0, gam = 0.0;
         if (VISC) {
-            const DevCase &P = m.cases[m.node_case[J]];
+            const DevCase &P = m.cases[ld_once(m.node_case + J)];
             prim_form = P.visc_model != VISC_REFERENCE;
             gop = P.gamma_over_Pr;
             gam = P.gamma;
@@ -585,13 +585,13 @@ __global__ void __launch_bounds__(256, 4) k_node_avg(const DevMesh m, const DevS
         // sequence the compiler can overlap (sums keep the reference order)
         int ci[kMaxCluster];
 #pragma unroll
-        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? m.cl[(int64_t)j * m.Nn + J] : -1;
+        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? ld_once(m.cl + (int64_t)j * m.Nn + J) : -1;
 #pragma unroll
         for (int j = 0; j < kMaxCluster; ++j)
-            if (ci[j] >= 0) add(ci[j], src[ci[j]], UNIT ? 1.0 : m.wt[(int64_t)j * m.Nn + J]);
+            if (ci[j] >= 0) add(ci[j], src[ci[j]], UNIT ? 1.0 : ld_once(m.wt + (int64_t)j * m.Nn + J));
         for (int j = kMaxCluster; j < W; ++j) {
-            const int c = m.cl[(int64_t)j * m.Nn + J];
-            if (c >= 0) add(c, src[c], UNIT ? 1.0 : m.wt[(int64_t)j * m.Nn + J]);
+            const int c = ld_once(m.cl + (int64_t)j * m.Nn + J);
+            if (c >= 0) add(c, src[c], UNIT ? 1.0 : ld_once(m.wt + (int64_t)j * m.Nn + J));
         }
         if (det != 0.0) { a0 = a0 / det; a1 = a1 / det; a2 = a2 / det; a3 = a3 / det; }
         s.nodeP[J] = zero_prims ? make_double4(0.0, 0.0, 0.0, 0.0) : make_double4(a0, a1, a2, a3);
@@ -630,14 +630,14 @@ __global__ void __launch_bounds__(256, 4) k_grad1_cells(const DevMesh m, const D
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         // padding cells have zero area (real ones are validated positive);
         // a triangle's fourth edge has zero length: no neighbour table read
-        const double area = m.area[g];
+        const double area = ld_once(m.area + g);
         if (area == 0.0) continue;
-        const int nf = (QUAD && m.len[3 * m.Nc + g] != 0.0) ? 4 : 3;
+        const int nf = (QUAD && ld_once(m.len + 3 * m.Nc + g) != 0.0) ? 4 : 3;
         double sx[3] = {0.0, 0.0, 0.0}, sy[3] = {0.0, 0.0, 0.0};
         for (int k = 0; k < nf; ++k) {
             const int64_t o = (int64_t)k * m.Nc + g;
-            const double side = m.len[o], nx = m.nx[o], ny = m.ny[o];
-            const int2 e = m.c2n[o];
+            const double side = ld_once(m.len + o), nx = ld_once(m.nx + o), ny = ld_once(m.ny + o);
+            const int2 e = ld_once(m.c2n + o);
             const double4 A = s.nodeC[e.x], B = s.nodeC[e.y];
             double fx, fy;
             fx = 0.5 * (A.x + B.x) * -ny * side; fy = 0.5 * (A.x + B.x) * -nx * side;
@@ -669,12 +669,12 @@ static __global__ void __launch_bounds__(256, 4) k_grad1_nodes(const DevMesh m, 
         };
         int ci[kMaxCluster];
 #pragma unroll
-        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? m.cl[(int64_t)j * m.Nn + J] : -1;
+        for (int j = 0; j < kMaxCluster; ++j) ci[j] = (j < W) ? ld_once(m.cl + (int64_t)j * m.Nn + J) : -1;
 #pragma unroll
         for (int j = 0; j < kMaxCluster; ++j)
             if (ci[j] >= 0) add(s.g1[ci[j]]);
         for (int j = kMaxCluster; j < W; ++j) {
-            const int c = m.cl[(int64_t)j * m.Nn + J];
+            const int c = ld_once(m.cl + (int64_t)j * m.Nn + J);
             if (c >= 0) add(s.g1[c]);
         }
         NodeGrad r;
