@@ -80,7 +80,7 @@ def make_params(cfg: Dict) -> N.Params:
     return p
 
 
-def make_launch(precision="f64", order="hilbert", loop="cell", block=0, node_block=0, persistent=0,
+def make_launch(precision="f64", order="hilbert", loop="tile", block=0, node_block=0, persistent=0,
                 graph_steps=0, stream=None, min_blocks=0, device=0) -> N.Launch:
     l = N.Launch()
     l.device = int(device)

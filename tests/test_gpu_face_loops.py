@@ -82,7 +82,7 @@ def test_tile_faces_equal_cell_loop(pkg, orc, case):
         from test_gpu_reference_mesh import shock_case
         mesh, cfg, prims = shock_case(pkg)
         n = 25
-    ref, href = gpu_state(pkg, mesh, cfg, prims, n)
+    ref, href = gpu_state(pkg, mesh, cfg, prims, n, loop="cell")
     got, hgot = gpu_state(pkg, mesh, cfg, prims, n, loop="tile")
     for k in ("Ucons", "prims", "node_prims"):
         assert np.array_equal(ref[k], got[k]), k
@@ -100,7 +100,7 @@ def test_tile_faces_batched_and_block128(pkg):
     meshes = [m for m, _, _ in items]
     cfgs = [c for _, c, _ in items]
     out = []
-    for launch in ({}, {"loop": "tile"}, {"loop": "tile", "block": 128}):
+    for launch in ({"loop": "cell"}, {"loop": "tile"}, {"loop": "tile", "block": 128}):
         s = pkg.solver.Solver(meshes, cfgs, pkg.solver.make_launch(**launch))
         for i, (_, _, p) in enumerate(items):
             s.createFields2d(i, *p)

@@ -29,7 +29,8 @@ def _run(pkg, mesh, cfg, prims, nsteps, **launch):
 @pytest.mark.parametrize("shape", [
     {"min_blocks": 2}, {"min_blocks": 4}, {"persistent": 1}, {"persistent": 1, "min_blocks": 4},
     {"node_block": 64}, {"node_block": 128}, {"block": 128}, {"graph_steps": 1}, {"graph_steps": 128},
-    {"loop": "tile"}, {"loop": "tile", "min_blocks": 2}, {"loop": "tile", "persistent": 1, "min_blocks": 4},
+    {"loop": "cell"}, {"loop": "cell", "min_blocks": 2}, {"loop": "tile", "min_blocks": 2},
+    {"loop": "tile", "persistent": 1, "min_blocks": 4},
 ])
 def test_launch_shape_is_bit_exact(pkg, shape):
     mesh, cfg, prims = _viscous_case(pkg)
