@@ -3,8 +3,9 @@ state update and reductions): error against the FP64 CPU oracle.
 
 Reported as the relative L2 and Linf error of rho, rho u, rho v, E after N
 steps and the drift of the conserved totals; the bounds below are the
-acceptance thresholds of this path (north star: density L2 error under 1e-5
-after 1000 steps on the cylinder; here shorter runs on smaller meshes).
+acceptance thresholds of this path (its target: density L2 error under
+1e-5 after 1000 steps on the 2.09M-cell cylinder; here shorter runs on
+smaller meshes).
 """
 import numpy as np
 import pytest

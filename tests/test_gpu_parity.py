@@ -1,7 +1,7 @@
 """GPU parity: the CUDA step through the C ABI against the CPU oracle.
 
-Tolerance (north star): FP64 within 1e-12 relative per step and 1e-10
-after 100 steps, measured per variable as max|gpu - oracle| / max|oracle|.
+Tolerance: FP64 within 1e-12 relative per step and 1e-10 after 100 steps,
+measured per variable as max|gpu - oracle| / max|oracle|.
 The FP64 kernels are built without multiply-add contraction, so most
 fields are expected to match bit for bit; the tests report that too.
 """
