@@ -3,7 +3,7 @@
  *
  * TEST INFRASTRUCTURE ONLY.  This file restates, in plain C, the FP64 CPU
  * algorithm of the reference solver (dimaZloy/2D-DNS-godunov-solver-, Julia)
- * so that the CUDA path can be checked against it.  It is the checker, never
+ * so that the CUDA path can be checked against it.  It is test infrastructure, never
  * the product: only tests/, __graft_entry__.smoke() and bench.py's CPU
  * baseline arm may load it.
  *
@@ -103,7 +103,7 @@ typedef struct {
     /* fields2d (primeObjects.jl:85-106) */
     double *densityCells, *UxCells, *UyCells, *pressureCells, *aSoundCells, *VMAXCells;
     double *densityNodes, *UxNodes, *UyNodes, *pressureNodes;
-    /* conservative work arrays of the driver (testInviscidFluxesGPUx32.jl:183-192) */
+    /* conservative work arrays of the reference top-level script (testInviscidFluxesGPUx32.jl:183-192) */
     double *UconsCellsOld, *UconsCellsNew, *UconsNodesOld, *UConsDiffCells, *Delta, *FLUXES;
     /* viscous work (calcDiffTerm.jl:37-62) and artificial viscosity */
     double *g1x[3], *g1y[3], *lap[3], *muArt, *dUdx, *dVdy;
@@ -984,7 +984,7 @@ void orc_run(orc_state *s, int32_t nsteps, orc_stats *last) {
     for (int32_t k = 0; k < nsteps; ++k) orc_step(s, last);
 }
 
-/* Field access for the checker: 0..5 cell primitives (rho,u,v,p,a,VMAX),
+/* Field access for the tests: 0..5 cell primitives (rho,u,v,p,a,VMAX),
  * 6..9 node primitives, 10 Uold, 11 Unew, 12 node conservatives, 13 Diff,
  * 14 Delta, 15 FLUXES, 16 artificial viscosity. */
 double *orc_field(orc_state *s, int32_t which) {

@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU oracle (godunov2d_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
-CPU-baseline arm of bench.py as the checker.  The product path never imports
+CPU-baseline arm of bench.py to check the CUDA path.  The product path never imports
 this module.  Parity of the oracle itself is unpinned by reference-produced
 vectors (the reference is Julia and records none); see the C file header.
 """
