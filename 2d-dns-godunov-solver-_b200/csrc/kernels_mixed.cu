@@ -8,6 +8,12 @@
 // reported against the FP64 oracle rather than asserted bit-exact.
 #include "mixed_face.cuh"
 
+// Register budget of the mixed node-side passes, as resident 256-thread
+// blocks per SM.
+#ifndef GD2D_NODE_MINB_MIXED
+#define GD2D_NODE_MINB_MIXED 6
+#endif
+
 namespace gd2d {
 
 namespace {
@@ -80,7 +86,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
 // Node-side kernels: gather-latency bound, registers capped for 6
 // resident blocks per SM.
 template <bool VISC, bool UNIT>
-__global__ void __launch_bounds__(256, 6) k_node_avg_mixed(const DevMesh m, const DevState s, int flip, int zero_prims,
+__global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_node_avg_mixed(const DevMesh m, const DevState s, int flip, int zero_prims,
                                                         int64_t n0, int64_t n1) {
     const int par = *s.parity;
     const float4 *__restrict__ src = s.primf + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
@@ -128,15 +134,12 @@ __global__ void __launch_bounds__(256, 6) k_node_avg_mixed(const DevMesh m, cons
         }
     }
     if (flip) {
-        __shared__ int s_last;
+        // Every warp of the block has read the parity once the barrier is
+        // passed; the block that completes the count flips it.  Nothing in
+        // this kernel reads what the others wrote, so no fence: stream order
+        // makes the flip and the node values visible to the next kernel.
         __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            unsigned int prev = atomicAdd(s.node_done, 1u);
-            s_last = (prev == gridDim.x - 1u) ? 1 : 0;
-        }
-        __syncthreads();
-        if (s_last && threadIdx.x == 0) {
+        if (threadIdx.x == 0 && atomicAdd(s.node_done, 1u) == gridDim.x - 1u) {
             *s.node_done = 0u;
             *s.parity = par ^ 1;
         }
@@ -144,7 +147,7 @@ __global__ void __launch_bounds__(256, 6) k_node_avg_mixed(const DevMesh m, cons
 }
 
 template <bool QUAD>
-__global__ void __launch_bounds__(256, 6) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
+__global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         // padding cells have zero area; triangles a zero-length fourth edge
         if (ld_once(m.areaf + g) == 0.f) continue;
@@ -168,7 +171,7 @@ __global__ void __launch_bounds__(256, 6) k_grad1_cells_mixed(const DevMesh m, c
     }
 }
 
-__global__ void __launch_bounds__(256, 6) k_grad1_nodes_mixed(const DevMesh m, const DevState s) {
+__global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_grad1_nodes_mixed(const DevMesh m, const DevState s) {
     const int W = m.cluster_w;
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};

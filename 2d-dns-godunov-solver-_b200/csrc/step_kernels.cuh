@@ -14,6 +14,11 @@
 #include "gd2d_internal.h"
 #include "physics.cuh"
 
+// Register budget of the node-side passes, as resident 256-thread blocks per SM.
+#ifndef GD2D_NODE_MINB
+#define GD2D_NODE_MINB 4
+#endif
+
 namespace gd2d {
 
 // Loads and stores of data a step touches once (per-cell and per-face mesh
@@ -549,7 +554,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
 // register budget is capped for 4 resident blocks per SM (more warps in
 // flight; measured faster than the unconstrained 76-register build).
 template <bool VISC, bool UNIT>
-__global__ void __launch_bounds__(256, 4) k_node_avg(const DevMesh m, const DevState s, int flip, int zero_prims,
+__global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_node_avg(const DevMesh m, const DevState s, int flip, int zero_prims,
                                                   int64_t n0, int64_t n1) {
     const int par = *s.parity;
     const double4 *__restrict__ src = s.prim + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
@@ -605,15 +610,12 @@ __global__ void __launch_bounds__(256, 4) k_node_avg(const DevMesh m, const DevS
         }
     }
     if (flip) {
-        __shared__ int s_last;
+        // Every warp of the block has read the parity once the barrier is
+        // passed; the block that completes the count flips it.  Nothing in
+        // this kernel reads what the others wrote, so no fence: stream order
+        // makes the flip and the node values visible to the next kernel.
         __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            unsigned int prev = atomicAdd(s.node_done, 1u);
-            s_last = (prev == gridDim.x - 1u) ? 1 : 0;
-        }
-        __syncthreads();
-        if (s_last && threadIdx.x == 0) {
+        if (threadIdx.x == 0 && atomicAdd(s.node_done, 1u) == gridDim.x - 1u) {
             *s.node_done = 0u;
             *s.parity = par ^ 1;
         }
@@ -626,7 +628,7 @@ __global__ void __launch_bounds__(256, 4) k_node_avg(const DevMesh m, const DevS
 // means (calcScalarFieldGreenGaussNodesBasedGradient, calcGradients.jl:36-139:
 // gradX pairs with -ny, gradY with -nx).
 template <bool QUAD>
-__global__ void __launch_bounds__(256, 4) k_grad1_cells(const DevMesh m, const DevState s) {
+__global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_grad1_cells(const DevMesh m, const DevState s) {
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         // padding cells have zero area (real ones are validated positive);
         // a triangle's fourth edge has zero length: no neighbour table read
@@ -657,7 +659,7 @@ __global__ void __launch_bounds__(256, 4) k_grad1_cells(const DevMesh m, const D
 
 // Unweighted node means of the first gradients (calcPhiInCellCluster on the
 // gradient fields, calcGradients.jl:3-18).
-static __global__ void __launch_bounds__(256, 4) k_grad1_nodes(const DevMesh m, const DevState s) {
+static __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_grad1_nodes(const DevMesh m, const DevState s) {
     const int W = m.cluster_w;
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};

@@ -121,6 +121,35 @@ def test_cylinder_sutherland_artvisc_venkat(pkg, orc):
     compare_stats(gh, oh, 1e-12)
 
 
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_edge_pairs_listed_end_first(pkg, orc, precision):
+    """cells2nodes may list an edge's node pair in either order: the viscous
+    passes average the pair as 0.5 (a + b), which is symmetric.  Listing the
+    pair of edge 0 end-first in every third cell must not change the state
+    by a single bit, and in FP64 it still matches the oracle."""
+    import dataclasses
+    mesh, cfg, prims = pkg.cases.cylinder_case(65, radius=0.5)
+    c2n = np.array(mesh.cells2nodes)
+    rows = np.arange(0, mesh.nCells, 3)
+    c2n[rows, 0], c2n[rows, 1] = mesh.cells2nodes[rows, 1], mesh.cells2nodes[rows, 0]
+    swapped = dataclasses.replace(mesh, cells2nodes=c2n)
+    out = []
+    for m in (mesh, swapped):
+        s = pkg.setupSolver(m, cfg, precision=precision)
+        s.createFields2d(0, *prims)
+        s.propagate2d(25)
+        out.append(s.get_state(0))
+        s.close()
+    for key in ("Ucons", "prims", "node_prims"):
+        assert np.array_equal(out[0][key], out[1][key]), key
+    if precision == "f64":
+        o = orc.Oracle(swapped, cfg, nthreads=4)
+        o.init_fields(*prims)
+        for _ in range(25):
+            o.step()
+        assert relerr(out[1]["Ucons"], o.field("Uold")) <= TOL_100
+
+
 @pytest.mark.parametrize("flux", ["roe", "ausm_m2020"])
 def test_other_fluxes(pkg, orc, flux):
     mesh, cfg, prims = pkg.cases.square_inviscid(41, flux=flux)
