@@ -100,7 +100,7 @@ struct gd2d_handle {
     double4 *split_unew = nullptr, *split_flux = nullptr, *split_delta = nullptr, *split_diff = nullptr;
     bool split_stage_done = false, split_diff_valid = false;
     std::vector<CaseState> cs_host;  // host copy: steps taken per case (advanced by propagate)
-    DevStats *ring_host = nullptr;    // page-locked copy of the statistics ring
+    DevStats *ring_host = nullptr;    // page-locked, mapped copy of the statistics ring
     std::string err;
 };
 
@@ -867,8 +867,13 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     cudaEventCreate(&h->ev_eager[0]);
     cudaEventCreate(&h->ev_eager[1]);
     {
-        cudaError_t e = cudaMallocHost((void **)&h->ring_host, sizeof(DevStats) * (size_t)s.ring_len * n_cases);
-        if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaMallocHost: %s", cudaGetErrorString(e)));
+        // mapped: each step's finalizing warp writes its statistics row here
+        // directly, so a step needs no copy before the host can read them
+        cudaError_t e = cudaHostAlloc((void **)&h->ring_host, sizeof(DevStats) * (size_t)s.ring_len * n_cases,
+                                      cudaHostAllocMapped);
+        if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_OOM, "cudaHostAlloc: %s", cudaGetErrorString(e)));
+        e = cudaHostGetDevicePointer((void **)&s.ring_host, h->ring_host, 0);
+        if (e != cudaSuccess) return bail(fail(h, GD2D_ERR_CUDA, "cudaHostGetDevicePointer: %s", cudaGetErrorString(e)));
     }
     // uploads above went through the legacy stream; finish them before any
     // work is queued on the handle's stream
@@ -888,26 +893,96 @@ static int copy_sync(gd2d_handle *h, void *dst, const void *src, size_t bytes, c
     return GD2D_OK;
 }
 
-// Host copy between a caller's array and the page-locked stage, split over
-// a few threads for large fields (one thread leaves most of the memory
-// bandwidth unused).
-static void host_copy(void *dst, const void *src, size_t bytes) {
+// Transfers between a caller's host columns and the device stage go
+// through the page-locked host stage in slices of >= 4 MB, one worker
+// thread per slice (at most 8): a worker's host copy and its slice's DMA
+// overlap the other workers' copies, and the copies together use more of
+// the host memory bandwidth than one thread can.  The stage holds a case's
+// 4 columns back to back, element v * n + i for row i of column v.
+static unsigned stage_workers(size_t bytes) {
     const size_t kPart = (size_t)4 << 20;
     unsigned nt = std::thread::hardware_concurrency();
     nt = std::max(1u, std::min(nt, 8u));
-    nt = (unsigned)std::min<size_t>(nt, std::max<size_t>(1, bytes / kPart));
-    if (nt <= 1) {
-        std::memcpy(dst, src, bytes);
-        return;
+    return (unsigned)std::min<size_t>(nt, std::max<size_t>(1, bytes / kPart));
+}
+
+// Elements [b0, b1) of the stage, copied from (to_stage) or to the columns.
+static void stage_copy(double *stage, double *const cols[4], int64_t n, size_t b0, size_t b1, bool to_stage) {
+    while (b0 < b1) {
+        const size_t v = b0 / (size_t)n, i = b0 % (size_t)n;
+        const size_t len = std::min(b1 - b0, (size_t)n - i);
+        if (to_stage) std::memcpy(stage + b0, cols[v] + i, sizeof(double) * len);
+        else std::memcpy(cols[v] + i, stage + b0, sizeof(double) * len);
+        b0 += len;
     }
-    std::vector<std::thread> th;
-    const size_t part = (bytes + nt - 1) / nt;
-    for (unsigned k = 0; k < nt; ++k) {
-        const size_t b0 = k * part, b1 = std::min(bytes, b0 + part);
-        if (b0 >= b1) break;
-        th.emplace_back([=] { std::memcpy((char *)dst + b0, (const char *)src + b0, b1 - b0); });
+}
+
+// Host columns -> h_stage -> d_stage (queued on the handle's stream).
+static int staged_upload(gd2d_handle *h, const double *const src[4], int64_t n) {
+    double *cols[4] = {const_cast<double *>(src[0]), const_cast<double *>(src[1]), const_cast<double *>(src[2]),
+                       const_cast<double *>(src[3])};
+    const size_t total = 4 * (size_t)n;
+    const unsigned nt = stage_workers(sizeof(double) * total);
+    std::vector<cudaError_t> err(nt, cudaSuccess);
+    auto work = [&](unsigned k) {
+        const size_t b0 = total * k / nt, b1 = total * (k + 1) / nt;
+        stage_copy(h->h_stage, cols, n, b0, b1, true);
+        if (nt > 1) err[k] = cudaSetDevice(h->device);
+        if (err[k] == cudaSuccess)
+            err[k] = cudaMemcpyAsync(h->d_stage + b0, h->h_stage + b0, sizeof(double) * (b1 - b0),
+                                     cudaMemcpyHostToDevice, h->stream);
+    };
+    if (nt == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned k = 0; k < nt; ++k) th.emplace_back(work, k);
+        for (auto &t : th) t.join();
     }
-    for (auto &t : th) t.join();
+    for (cudaError_t e : err)
+        if (e != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "staged upload: %s", cudaGetErrorString(e));
+    return GD2D_OK;
+}
+
+// d_stage -> h_stage -> a column-major (n, 4) host matrix; returns when the
+// matrix is complete.
+static int staged_download(gd2d_handle *h, double *dst, int64_t n) {
+    double *cols[4] = {dst, dst + n, dst + 2 * n, dst + 3 * n};
+    const size_t total = 4 * (size_t)n;
+    const unsigned nt = stage_workers(sizeof(double) * total);
+    std::vector<cudaEvent_t> ev(nt, nullptr);
+    cudaError_t e = cudaSuccess;
+    for (unsigned k = 0; k < nt && e == cudaSuccess; ++k) {
+        const size_t b0 = total * k / nt, b1 = total * (k + 1) / nt;
+        e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h->h_stage + b0, h->d_stage + b0, sizeof(double) * (b1 - b0), cudaMemcpyDeviceToHost,
+                                h->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k], h->stream);
+    }
+    std::vector<cudaError_t> err(nt, e);
+    if (e == cudaSuccess) {
+        auto work = [&](unsigned k) {
+            const size_t b0 = total * k / nt, b1 = total * (k + 1) / nt;
+            if (nt > 1) err[k] = cudaSetDevice(h->device);
+            if (err[k] == cudaSuccess) err[k] = cudaEventSynchronize(ev[k]);
+            if (err[k] == cudaSuccess) stage_copy(h->h_stage, cols, n, b0, b1, false);
+        };
+        if (nt == 1) {
+            work(0);
+        } else {
+            std::vector<std::thread> th;
+            for (unsigned k = 0; k < nt; ++k) th.emplace_back(work, k);
+            for (auto &t : th) t.join();
+        }
+    } else {
+        cudaStreamSynchronize(h->stream);  // nothing queued above may outlive the call
+    }
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    for (cudaError_t x : err)
+        if (x != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "staged download: %s", cudaGetErrorString(x));
+    return GD2D_OK;
 }
 
 static int ensure_case(gd2d_handle *h, int32_t icase) {
@@ -982,11 +1057,9 @@ int gd2d_set_state(gd2d_handle *h, int32_t icase, const double *density, const d
     double4 *dst = nullptr;
     if ((rc = case_prims_dst(h, icase, &dst))) return rc;
     const int64_t n = hc.nc;
-    double *st = h->d_stage;
     const double *cols[4] = {density, ux, uy, pressure};
-    for (int v = 0; v < 4; ++v) host_copy(h->h_stage + v * n, cols[v], sizeof(double) * n);
-    CUDA_TRY(h, cudaMemcpyAsync(st, h->h_stage, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, h->stream));
-    CUDA_TRY(h, launch_cols_to_dev(st, h->d_perm + hc.cell_off, n, dst, h->stream));
+    if ((rc = staged_upload(h, cols, n))) return rc;
+    CUDA_TRY(h, launch_cols_to_dev(h->d_stage, h->d_perm + hc.cell_off, n, dst, h->stream));
     return init_case(h, icase, hc.start_time, hc.params.init_nodes != 0);
 }
 
@@ -999,8 +1072,8 @@ int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, do
     double4 *dst = nullptr;
     if ((rc = case_prims_dst(h, icase, &dst))) return rc;
     const int64_t n = hc.nc;
-    host_copy(h->h_stage, ucons, sizeof(double) * 4 * n);
-    CUDA_TRY(h, cudaMemcpyAsync(h->d_stage, h->h_stage, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, h->stream));
+    const double *cols[4] = {ucons, ucons + n, ucons + 2 * n, ucons + 3 * n};
+    if ((rc = staged_upload(h, cols, n))) return rc;
     CUDA_TRY(h, launch_cons_to_prims(h->d_stage, h->d_perm + hc.cell_off, n, hc.params.Gamma, dst, h->stream));
     return init_case(h, icase, flow_time, rebuild_nodes != 0, h->d_stage);
 }
@@ -1104,11 +1177,7 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
         // steps taken so far per case, kept on the host (the device's copy
         // advances in step with it): no read-back before the launches
         std::vector<int64_t> step0(h->ncases);
-        bool lockstep = true;
-        for (int c = 0; c < h->ncases; ++c) {
-            step0[c] = h->cs_host[c].step;
-            lockstep &= step0[c] == step0[0];
-        }
+        for (int c = 0; c < h->ncases; ++c) step0[c] = h->cs_host[c].step;
         // graphs this chunk needs, captured before the timed window opens
         if (G > 1 && chunk >= G && !h->graph) {
             int rc = capture_graph(h, G, timing);
@@ -1140,21 +1209,9 @@ int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
             launches += kernels_per_step(h);
         }
         CUDA_TRY(h, cudaEventRecord(h->ev_total[1], h->stream));
-        // the chunk's statistics rows (the ring is [ring_len][ncases], rows
-        // wrap; cases whose step counts differ -- one re-initialised in mid
-        // run -- sit in different rows, then the whole ring is read)
-        if (lockstep) {
-            const int64_t r0 = step0[0] % RL;
-            const int64_t first = std::min<int64_t>(chunk, RL - r0);
-            CUDA_TRY(h, cudaMemcpyAsync(h->ring_host + r0 * h->ncases, h->s.ring + r0 * h->ncases,
-                                        sizeof(DevStats) * first * h->ncases, cudaMemcpyDeviceToHost, h->stream));
-            if (first < chunk)
-                CUDA_TRY(h, cudaMemcpyAsync(h->ring_host, h->s.ring, sizeof(DevStats) * (chunk - first) * h->ncases,
-                                            cudaMemcpyDeviceToHost, h->stream));
-        } else {
-            CUDA_TRY(h, cudaMemcpyAsync(h->ring_host, h->s.ring, sizeof(DevStats) * RL * h->ncases,
-                                        cudaMemcpyDeviceToHost, h->stream));
-        }
+        // the chunk's statistics rows are in the mapped ring once the stream
+        // is idle (rows are [ring_len][ncases] and wrap; every case steps in
+        // every launch, so each case's rows of this chunk are fresh)
         CUDA_TRY(h, cudaStreamSynchronize(h->stream));
         float ms = 0.f;
         cudaEventElapsedTime(&ms, h->ev_total[0], h->ev_total[1]);
@@ -1216,10 +1273,7 @@ static int download_rows(gd2d_handle *h, const double4 *src, const float4 *srcf,
     if (!dst) return GD2D_OK;
     CUDA_TRY(h, srcf ? launch_dev_to_cols_f(srcf, inv, n, h->d_stage, h->stream)
                      : launch_dev_to_cols(src, inv, n, h->d_stage, h->stream));
-    CUDA_TRY(h, cudaMemcpyAsync(h->h_stage, h->d_stage, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, h->stream));
-    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-    host_copy(dst, h->h_stage, sizeof(double) * 4 * n);
-    return GD2D_OK;
+    return staged_download(h, dst, n);
 }
 
 int gd2d_get_state(gd2d_handle *h, int32_t icase, double *ucons, double *prims, double *node_prims) {

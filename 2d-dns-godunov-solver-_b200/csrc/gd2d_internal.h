@@ -146,6 +146,7 @@ struct DevState {
     unsigned int *group_done;  // [ngroups] tiles of the group finished this step
     CaseState *cstate; // [ncases]
     DevStats *ring;    // [ring_len][ncases]
+    DevStats *ring_host;  // the host's page-locked, mapped copy of ring, written alongside it
     int32_t *parity;   // step parity (which prim buffer is current)
     unsigned int *node_done;
     int32_t ring_len;

@@ -153,7 +153,9 @@ static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c,
             st.step = cs->step + 1;
             st.nonfinite = acc.bad > 0.0 ? 1 : 0;
             st.reserved0 = 0;
-            s.ring[(cs->step % s.ring_len) * m.ncases + c] = st;
+            const int64_t row = (cs->step % s.ring_len) * m.ncases + c;
+            s.ring[row] = st;
+            s.ring_host[row] = st;  // over PCIe: the host reads it after the stream's sync
             cs->t = cs->t + cs->dt;
             cs->step = cs->step + 1;
             if (acc.bad > 0.0) cs->nonfinite = 1;
