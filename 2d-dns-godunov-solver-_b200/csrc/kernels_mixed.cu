@@ -148,21 +148,33 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_node_avg_mixed(co
 
 template <bool QUAD>
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
+    constexpr int NF = QUAD ? 4 : 3;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
-        // padding cells have zero area; triangles a zero-length fourth edge
-        if (ld_once(m.areaf + g) == 0.f) continue;
-        const int nf = (QUAD && ld_once(m.lenf + 3 * m.Nc + g) != 0.f) ? 4 : 3;
-        float sx[3] = {0.f, 0.f, 0.f}, sy[3] = {0.f, 0.f, 0.f};
-        for (int k = 0; k < nf; ++k) {
+        // all per-cell loads first (two trips to memory per cell); padding
+        // cells have zero area and are dropped at the store, triangles have
+        // a zero-length fourth edge
+        const float area = ld_once(m.areaf + g), rA = ld_once(m.rareaf + g);
+        float side[NF], nx[NF], ny[NF];
+        int2 e[NF];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
             const int64_t o = (int64_t)k * m.Nc + g;
-            const float side = ld_once(m.lenf + o), nx = ld_once(m.nxf + o), ny = ld_once(m.nyf + o);
-            const int2 e = ld_once(m.c2n + o);
-            const float4 A = s.nodeCf[e.x], B = s.nodeCf[e.y];
-            sx[0] += 0.5f * (A.x + B.x) * -ny * side; sy[0] += 0.5f * (A.x + B.x) * -nx * side;
-            sx[1] += 0.5f * (A.y + B.y) * -ny * side; sy[1] += 0.5f * (A.y + B.y) * -nx * side;
-            sx[2] += 0.5f * (A.z + B.z) * -ny * side; sy[2] += 0.5f * (A.z + B.z) * -nx * side;
+            side[k] = ld_once(m.lenf + o);
+            nx[k] = ld_once(m.nxf + o);
+            ny[k] = ld_once(m.nyf + o);
+            e[k] = ld_once(m.c2n + o);
         }
-        const float rA = ld_once(m.rareaf + g);
+        const int nf = (QUAD && side[NF - 1] != 0.f) ? 4 : 3;
+        float sx[3] = {0.f, 0.f, 0.f}, sy[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
+            if (k >= nf) break;
+            const float4 A = s.nodeCf[e[k].x], B = s.nodeCf[e[k].y];
+            sx[0] += 0.5f * (A.x + B.x) * -ny[k] * side[k]; sy[0] += 0.5f * (A.x + B.x) * -nx[k] * side[k];
+            sx[1] += 0.5f * (A.y + B.y) * -ny[k] * side[k]; sy[1] += 0.5f * (A.y + B.y) * -nx[k] * side[k];
+            sx[2] += 0.5f * (A.z + B.z) * -ny[k] * side[k]; sy[2] += 0.5f * (A.z + B.z) * -nx[k] * side[k];
+        }
+        if (area == 0.f) continue;
         NodeGradF r;
         r.ru = make_float2(sx[0] * rA, sy[0] * rA);
         r.rv = make_float2(sx[1] * rA, sy[1] * rA);

@@ -631,26 +631,38 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_node_avg(const DevMesh 
 // gradX pairs with -ny, gradY with -nx).
 template <bool QUAD>
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_grad1_cells(const DevMesh m, const DevState s) {
+    constexpr int NF = QUAD ? 4 : 3;
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
-        // padding cells have zero area (real ones are validated positive);
-        // a triangle's fourth edge has zero length: no neighbour table read
+        // Every per-cell load is issued before any of them is tested, so a
+        // cell costs two trips to memory (its own arrays, then the node
+        // gathers).  Padding cells (zero area, node 0 in their edge slots)
+        // are dropped at the store; a triangle's fourth edge has zero length.
         const double area = ld_once(m.area + g);
-        if (area == 0.0) continue;
-        const int nf = (QUAD && ld_once(m.len + 3 * m.Nc + g) != 0.0) ? 4 : 3;
-        double sx[3] = {0.0, 0.0, 0.0}, sy[3] = {0.0, 0.0, 0.0};
-        for (int k = 0; k < nf; ++k) {
+        double side[NF], nx[NF], ny[NF];
+        int2 e[NF];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
             const int64_t o = (int64_t)k * m.Nc + g;
-            const double side = ld_once(m.len + o), nx = ld_once(m.nx + o), ny = ld_once(m.ny + o);
-            const int2 e = ld_once(m.c2n + o);
-            const double4 A = s.nodeC[e.x], B = s.nodeC[e.y];
+            side[k] = ld_once(m.len + o);
+            nx[k] = ld_once(m.nx + o);
+            ny[k] = ld_once(m.ny + o);
+            e[k] = ld_once(m.c2n + o);
+        }
+        const int nf = (QUAD && side[NF - 1] != 0.0) ? 4 : 3;
+        double sx[3] = {0.0, 0.0, 0.0}, sy[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
+            if (k >= nf) break;
+            const double4 A = s.nodeC[e[k].x], B = s.nodeC[e[k].y];
             double fx, fy;
-            fx = 0.5 * (A.x + B.x) * -ny * side; fy = 0.5 * (A.x + B.x) * -nx * side;
+            fx = 0.5 * (A.x + B.x) * -ny[k] * side[k]; fy = 0.5 * (A.x + B.x) * -nx[k] * side[k];
             sx[0] = (k == 0) ? fx : sx[0] + fx; sy[0] = (k == 0) ? fy : sy[0] + fy;
-            fx = 0.5 * (A.y + B.y) * -ny * side; fy = 0.5 * (A.y + B.y) * -nx * side;
+            fx = 0.5 * (A.y + B.y) * -ny[k] * side[k]; fy = 0.5 * (A.y + B.y) * -nx[k] * side[k];
             sx[1] = (k == 0) ? fx : sx[1] + fx; sy[1] = (k == 0) ? fy : sy[1] + fy;
-            fx = 0.5 * (A.z + B.z) * -ny * side; fy = 0.5 * (A.z + B.z) * -nx * side;
+            fx = 0.5 * (A.z + B.z) * -ny[k] * side[k]; fy = 0.5 * (A.z + B.z) * -nx[k] * side[k];
             sx[2] = (k == 0) ? fx : sx[2] + fx; sy[2] = (k == 0) ? fy : sy[2] + fy;
         }
+        if (area == 0.0) continue;
         NodeGrad r;
         r.ru = make_double2(sx[0] / area, sy[0] / area);
         r.rv = make_double2(sx[1] / area, sy[1] / area);
