@@ -81,7 +81,9 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
         const int4 nb = ld_once(m.nbr + g);
         const bool is_quad = QUAD && (nb.w != kAbsent);
         float diff[4] = {0.f, 0.f, 0.f, 0.f};
-        if (VISC && nb.x != kAbsent) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
+        // triangles: evaluated for padding cells too (node 0 in their edge
+        // slots; the result is unused), so its loads need not wait for nb
+        if (VISC && (!QUAD || nb.x != kAbsent)) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
         __syncthreads();
         Part part;
         part.init();
