@@ -165,12 +165,13 @@ __device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &
 // (calcOneStageMUSCLcpuFast.jl:94-99), the densityConstrained clamp, the
 // primitives recovered from the FP64 state (evaluate2d.jl:87-104) and the
 // cell's contribution to the step's reductions.
+// U and rarea are the cell's state and inverse area, loaded by the caller
+// (the tile kernel issues those loads before its flux barrier).
 __device__ __forceinline__ void cell_update_mixed(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
                                                   const float4 &me, const float *F, const float *diff, double dt,
-                                                  float4 *__restrict__ pout, Part &part) {
+                                                  const double4 &U, float rarea, float4 *__restrict__ pout,
+                                                  Part &part) {
     const float bdt = (float)(P.beta * dt);
-    const float rarea = ld_once(m.rareaf + g);
-    const double4 U = ld_once(s.U + g);
     const double Uo[4] = {U.x, U.y, U.z, U.w};
     double Un[4];
 #pragma unroll

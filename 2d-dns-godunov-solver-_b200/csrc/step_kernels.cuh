@@ -366,11 +366,11 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
 // Euler update (calcOneStageMUSCLcpuFast.jl:94-99), the densityConstrained
 // clamp (evaluate2d.jl:63-77), updateVariablesSA (evaluate2d.jl:87-104) and
 // the cell's contribution to the step's reductions.
+// U and rarea are the cell's state and inverse area, loaded by the caller
+// (the tile kernel issues those loads before its flux barrier).
 __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
                                             const double4 &me, const double *F, const double *diff, double dt,
-                                            double4 *__restrict__ pout, Part &part) {
-    const double rarea = ld_once(m.rarea + g);
-    const double4 U = ld_once(s.U + g);
+                                            const double4 &U, double rarea, double4 *__restrict__ pout, Part &part) {
     const double Uo[4] = {U.x, U.y, U.z, U.w};
     double Un[4];
 #pragma unroll
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const 
             }
             double diff[4] = {0.0, 0.0, 0.0, 0.0};
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
-            cell_update(m, s, P, g, me, F, diff, dt, pout, part);
+            cell_update(m, s, P, g, me, F, diff, dt, ld_once(s.U + g), ld_once(m.rarea + g), pout, part);
         }
         tile_epilogue(m, s, tile, c, part, s_red, false);
     }
@@ -529,6 +529,10 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
         const bool is_quad = QUAD && (nb.w != kAbsent);
         double diff[4] = {0.0, 0.0, 0.0, 0.0};
         if (VISC && nb.x != kAbsent) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
+        // the update's own loads go out before the barrier (padded arrays:
+        // in bounds for padding cells, whose values are not used)
+        const double4 U = ld_once(s.U + g);
+        const double rarea = ld_once(m.rarea + g);
         __syncthreads();
         Part part;
         part.init();
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
                 const double4 a3 = s_flux[NS - 1][threadIdx.x];
                 F[0] = F[0] + a3.x; F[1] = F[1] + a3.y; F[2] = F[2] + a3.z; F[3] = F[3] + a3.w;
             }
-            cell_update(m, s, P, g, me, F, diff, dt, pout, part);
+            cell_update(m, s, P, g, me, F, diff, dt, U, rarea, pout, part);
         }
         tile_epilogue(m, s, tile, c, part, s_red, false);
     }
@@ -820,7 +824,7 @@ __global__ void __launch_bounds__(256, MINB) k_face_update(const DevMesh m, cons
             }
             double diff[4] = {0.0, 0.0, 0.0, 0.0};
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
-            cell_update(m, s, P, g, me, F, diff, dt, pout, part);
+            cell_update(m, s, P, g, me, F, diff, dt, ld_once(s.U + g), ld_once(m.rarea + g), pout, part);
         }
         tile_epilogue(m, s, tile, c, part, s_red, false);
     }
