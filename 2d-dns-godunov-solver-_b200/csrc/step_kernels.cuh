@@ -480,19 +480,22 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
     double4 *__restrict__ pout = s.prim + (int64_t)(par ^ 1) * m.Nc;
     const int B = blockDim.x;
     for (int64_t tile = blockIdx.x; tile < m.ntiles; tile += gridDim.x) {
+        const int64_t base = tile * B;
+        const int64_t g = base + threadIdx.x;
+        // loads that depend on nothing go out first: the face-list bounds
+        // and HX (used only with the Venkatakrishnan limiter) need not wait
+        // for the case record
+        const int64_t f0 = m.tf_off[tile], f1 = m.tf_off[tile + 1];
+        s_prim[threadIdx.x] = pin[g];
+        s_hx[threadIdx.x] = ld_once(m.hx + g);
         const int c = m.tile_case[tile];
         const DevCase &P = m.cases[c];
         const double t = s.cstate[c].t;
-        const int64_t base = tile * B;
-        const int64_t g = base + threadIdx.x;
         const bool venkat = P.limiter == LIM_VENKAT;
-        s_prim[threadIdx.x] = pin[g];
-        if (venkat) s_hx[threadIdx.x] = ld_once(m.hx + g);
         __syncthreads();
         const double gam = P.gamma;
         const double g2 = 2.0 * (gam - 1.0) / (gam + 1.0);
-        const int64_t f1 = m.tf_off[tile + 1];
-        for (int64_t f = m.tf_off[tile] + threadIdx.x; f < f1; f += B) {
+        for (int64_t f = f0 + threadIdx.x; f < f1; f += B) {
             const int4 rec = ld_once(m.tf_rec + f);
             const TileFace tf = unpack_tile_face(rec.y);
             const double4 a4 = s_prim[tf.la];
