@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
             }
             float diff[4] = {0.f, 0.f, 0.f, 0.f};
             if (VISC) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
-            cell_update_mixed(m, s, P, g, me, F, diff, dt, ld_once(s.U + g), ld_once(m.rareaf + g), pout, part);
+            cell_update_mixed(m, s, P, g, me, F, diff, dt, load_cell_in_f(m, s, g), pout, part);
         }
         tile_epilogue(m, s, tile, c, part, s_red, false);
     }

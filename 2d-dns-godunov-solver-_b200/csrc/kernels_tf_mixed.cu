@@ -89,8 +89,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
         if (VISC && (!QUAD || nb.x != kAbsent)) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
         // the update's own loads go out before the barrier (padded arrays:
         // in bounds for padding cells, whose values are not used)
-        const double4 U = ld_once(s.U + g);
-        const float rarea = ld_once(m.rareaf + g);
+        const CellInF cin = load_cell_in_f(m, s, g);
         __syncthreads();
         Part part;
         part.init();
@@ -101,7 +100,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
                 const float4 a3 = s_flux[NS - 1][threadIdx.x];
                 F[0] += a3.x; F[1] += a3.y; F[2] += a3.z; F[3] += a3.w;
             }
-            cell_update_mixed(m, s, P, g, me, F, diff, dt, U, rarea, pout, part);
+            cell_update_mixed(m, s, P, g, me, F, diff, dt, cin, pout, part);
         }
         tile_epilogue(m, s, tile, c, part, s_red, false);
     }

@@ -165,13 +165,27 @@ __device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &
 // (calcOneStageMUSCLcpuFast.jl:94-99), the densityConstrained clamp, the
 // primitives recovered from the FP64 state (evaluate2d.jl:87-104) and the
 // cell's contribution to the step's reductions.
-// U and rarea are the cell's state and inverse area, loaded by the caller
-// (the tile kernel issues those loads before its flux barrier).
+// The per-cell arrays the update reads, loaded by the caller (the tile
+// kernel issues these loads before its flux barrier).
+struct CellInF {
+    double4 U;  // FP64 conservative state before the step
+    float rarea, area, charlen;
+};
+__device__ __forceinline__ CellInF load_cell_in_f(const DevMesh &m, const DevState &s, int64_t g) {
+    CellInF r;
+    r.U = ld_once(s.U + g);
+    r.rarea = ld_once(m.rareaf + g);
+    r.area = ld_once(m.areaf + g);
+    r.charlen = ld_once(m.charlenf + g);
+    return r;
+}
+
 __device__ __forceinline__ void cell_update_mixed(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
                                                   const float4 &me, const float *F, const float *diff, double dt,
-                                                  const double4 &U, float rarea, float4 *__restrict__ pout,
-                                                  Part &part) {
+                                                  const CellInF &in, float4 *__restrict__ pout, Part &part) {
     const float bdt = (float)(P.beta * dt);
+    const double4 U = in.U;
+    const float rarea = in.rarea;
     const double Uo[4] = {U.x, U.y, U.z, U.w};
     double Un[4];
 #pragma unroll
@@ -189,7 +203,7 @@ __device__ __forceinline__ void cell_update_mixed(const DevMesh &m, const DevSta
     const float a = sqrtf((float)(P.gamma * p * rinv));
     const float vmax = sqrtf((float)(ux * ux + uy * uy)) + a;
     pout[g] = make_float4((float)rho, (float)ux, (float)uy, (float)p);
-    const double area = (double)ld_once(m.areaf + g);
+    const double area = (double)in.area;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
         const double d = Un[v] - Uo[v];
@@ -198,7 +212,7 @@ __device__ __forceinline__ void cell_update_mixed(const DevMesh &m, const DevSta
     }
     part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
     part.vmax = (double)vmax;
-    part.rmin = (double)(ld_once(m.charlenf + g) / vmax);
+    part.rmin = (double)(in.charlen / vmax);
     part.rhomin = (double)me.x;
     part.rhomax = (double)me.x;
     const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&

@@ -366,11 +366,26 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
 // Euler update (calcOneStageMUSCLcpuFast.jl:94-99), the densityConstrained
 // clamp (evaluate2d.jl:63-77), updateVariablesSA (evaluate2d.jl:87-104) and
 // the cell's contribution to the step's reductions.
-// U and rarea are the cell's state and inverse area, loaded by the caller
-// (the tile kernel issues those loads before its flux barrier).
+// The per-cell arrays the update reads, loaded by the caller (the tile
+// kernel issues these loads before its flux barrier).
+struct CellIn {
+    double4 U;  // conservative state before the step
+    double rarea, area, charlen;
+};
+__device__ __forceinline__ CellIn load_cell_in(const DevMesh &m, const DevState &s, int64_t g) {
+    CellIn r;
+    r.U = ld_once(s.U + g);
+    r.rarea = ld_once(m.rarea + g);
+    r.area = ld_once(m.area + g);
+    r.charlen = ld_once(m.charlen + g);
+    return r;
+}
+
 __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
                                             const double4 &me, const double *F, const double *diff, double dt,
-                                            const double4 &U, double rarea, double4 *__restrict__ pout, Part &part) {
+                                            const CellIn &in, double4 *__restrict__ pout, Part &part) {
+    const double4 U = in.U;
+    const double rarea = in.rarea;
     const double Uo[4] = {U.x, U.y, U.z, U.w};
     double Un[4];
 #pragma unroll
@@ -388,7 +403,7 @@ __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s,
     const double a = sqrt(gam * p / rho);
     const double vmax = sqrt(ux * ux + uy * uy) + a;
     pout[g] = make_double4(rho, ux, uy, p);
-    const double area = ld_once(m.area + g);
+    const double area = in.area;
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
         const double d = Un[v] - Uo[v];
@@ -397,7 +412,7 @@ __device__ __forceinline__ void cell_update(const DevMesh &m, const DevState &s,
     }
     part.ek = 0.5 * rho * (ux * ux + uy * uy) * area;
     part.vmax = vmax;
-    part.rmin = ld_once(m.charlen + g) / vmax;
+    part.rmin = in.charlen / vmax;
     part.rhomin = me.x;
     part.rhomax = me.x;
     const bool ok = isfinite(Un[0]) && isfinite(Un[1]) && isfinite(Un[2]) && isfinite(Un[3]) && (rho > 0.0) &&
@@ -447,7 +462,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const 
             }
             double diff[4] = {0.0, 0.0, 0.0, 0.0};
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
-            cell_update(m, s, P, g, me, F, diff, dt, ld_once(s.U + g), ld_once(m.rarea + g), pout, part);
+            cell_update(m, s, P, g, me, F, diff, dt, load_cell_in(m, s, g), pout, part);
         }
         tile_epilogue(m, s, tile, c, part, s_red, false);
     }
@@ -534,8 +549,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
         if (VISC && nb.x != kAbsent) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
         // the update's own loads go out before the barrier (padded arrays:
         // in bounds for padding cells, whose values are not used)
-        const double4 U = ld_once(s.U + g);
-        const double rarea = ld_once(m.rarea + g);
+        const CellIn cin = load_cell_in(m, s, g);
         __syncthreads();
         Part part;
         part.init();
@@ -547,7 +561,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
                 const double4 a3 = s_flux[NS - 1][threadIdx.x];
                 F[0] = F[0] + a3.x; F[1] = F[1] + a3.y; F[2] = F[2] + a3.z; F[3] = F[3] + a3.w;
             }
-            cell_update(m, s, P, g, me, F, diff, dt, U, rarea, pout, part);
+            cell_update(m, s, P, g, me, F, diff, dt, cin, pout, part);
         }
         tile_epilogue(m, s, tile, c, part, s_red, false);
     }
@@ -827,7 +841,7 @@ __global__ void __launch_bounds__(256, MINB) k_face_update(const DevMesh m, cons
             }
             double diff[4] = {0.0, 0.0, 0.0, 0.0};
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
-            cell_update(m, s, P, g, me, F, diff, dt, ld_once(s.U + g), ld_once(m.rarea + g), pout, part);
+            cell_update(m, s, P, g, me, F, diff, dt, load_cell_in(m, s, g), pout, part);
         }
         tile_epilogue(m, s, tile, c, part, s_red, false);
     }
