@@ -170,6 +170,26 @@ struct LaunchCfg {
 // Message reported by gd2d_last_error(NULL) for calls without a handle.
 void set_handleless_error(const char *msg);
 
+// Launch of a step kernel as a programmatic dependent of the kernel before
+// it on the stream: it may be scheduled once every block of that kernel has
+// started (each calls pdl_trigger first), and its threads wait in pdl_wait
+// until that kernel has finished and its writes are visible.  This hides
+// the launch gap and fills the last wave of one step kernel with the next.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_dependent(void (*kernel)(KArgs...), int grid, int block, cudaStream_t st, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Launchers implemented in kernels_f64.cu.
 cudaError_t launch_cell_step_f64(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
                                  const LaunchCfg &lc, cudaStream_t st);

@@ -49,23 +49,19 @@ cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, 
     const int grid = grid_for(n1 - n0, b);
     const bool unit = m.unit_weights != 0;
     if (visc) {
-        if (unit) k_node_avg<true, true><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
-        else k_node_avg<true, false><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
-    } else {
-        if (unit) k_node_avg<false, true><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
-        else k_node_avg<false, false><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+        if (unit) return launch_dependent(k_node_avg<true, true>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
+        return launch_dependent(k_node_avg<true, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
     }
-    return cudaGetLastError();
+    if (unit) return launch_dependent(k_node_avg<false, true>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
+    return launch_dependent(k_node_avg<false, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
 }
 
 cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
     const int b = lc.node_block;
-    if (m.nfmax == 4) k_grad1_cells<true><<<grid_for(m.Nc, b), b, 0, st>>>(m, s);
-    else k_grad1_cells<false><<<grid_for(m.Nc, b), b, 0, st>>>(m, s);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = (m.nfmax == 4) ? launch_dependent(k_grad1_cells<true>, grid_for(m.Nc, b), b, st, m, s)
+                                   : launch_dependent(k_grad1_cells<false>, grid_for(m.Nc, b), b, st, m, s);
     if (e != cudaSuccess) return e;
-    k_grad1_nodes<<<grid_for(m.Nn, b), b, 0, st>>>(m, s);
-    return cudaGetLastError();
+    return launch_dependent(k_grad1_nodes, grid_for(m.Nn, b), b, st, m, s);
 }
 
 cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,

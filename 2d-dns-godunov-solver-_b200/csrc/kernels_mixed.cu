@@ -88,6 +88,8 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
 template <bool VISC, bool UNIT>
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_node_avg_mixed(const DevMesh m, const DevState s, int flip, int zero_prims,
                                                         int64_t n0, int64_t n1) {
+    pdl_trigger();
+    pdl_wait();
     const int par = *s.parity;
     const float4 *__restrict__ src = s.primf + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
     const int W = m.cluster_w;
@@ -149,6 +151,8 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_node_avg_mixed(co
 template <bool QUAD>
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_grad1_cells_mixed(const DevMesh m, const DevState s) {
     constexpr int NF = QUAD ? 4 : 3;
+    pdl_trigger();
+    pdl_wait();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         // all per-cell loads first (two trips to memory per cell); padding
         // cells have zero area and are dropped at the store, triangles have
@@ -185,6 +189,8 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_grad1_cells_mixed
 
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_grad1_nodes_mixed(const DevMesh m, const DevState s) {
     const int W = m.cluster_w;
+    pdl_trigger();
+    pdl_wait();
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int cnt = 0;
@@ -279,23 +285,19 @@ cudaError_t launch_node_avg_mixed(const DevMesh &m, const DevState &s, bool visc
     const int grid = grid_for_m(n1 - n0, b);
     const bool unit = m.unit_weights != 0;
     if (visc) {
-        if (unit) k_node_avg_mixed<true, true><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
-        else k_node_avg_mixed<true, false><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
-    } else {
-        if (unit) k_node_avg_mixed<false, true><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
-        else k_node_avg_mixed<false, false><<<grid, b, 0, st>>>(m, s, flip_parity, zero_prims, n0, n1);
+        if (unit) return launch_dependent(k_node_avg_mixed<true, true>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
+        return launch_dependent(k_node_avg_mixed<true, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
     }
-    return cudaGetLastError();
+    if (unit) return launch_dependent(k_node_avg_mixed<false, true>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
+    return launch_dependent(k_node_avg_mixed<false, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
 }
 
 cudaError_t launch_visc_grad_mixed(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
     const int b = lc.node_block;
-    if (m.nfmax == 4) k_grad1_cells_mixed<true><<<grid_for_m(m.Nc, b), b, 0, st>>>(m, s);
-    else k_grad1_cells_mixed<false><<<grid_for_m(m.Nc, b), b, 0, st>>>(m, s);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = (m.nfmax == 4) ? launch_dependent(k_grad1_cells_mixed<true>, grid_for_m(m.Nc, b), b, st, m, s)
+                                   : launch_dependent(k_grad1_cells_mixed<false>, grid_for_m(m.Nc, b), b, st, m, s);
     if (e != cudaSuccess) return e;
-    k_grad1_nodes_mixed<<<grid_for_m(m.Nn, b), b, 0, st>>>(m, s);
-    return cudaGetLastError();
+    return launch_dependent(k_grad1_nodes_mixed, grid_for_m(m.Nn, b), b, st, m, s);
 }
 
 cudaError_t launch_init_state_mixed(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,

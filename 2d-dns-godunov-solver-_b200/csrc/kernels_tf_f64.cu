@@ -10,10 +10,9 @@ namespace {
 template <int FLUX, bool VISC, bool QUAD>
 cudaError_t cell_step_tf(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
     const int grid = lc.persistent ? lc.grid : (int)m.ntiles;
-    if (lc.min_blocks >= 4) k_cell_step_tf<FLUX, VISC, QUAD, 4><<<grid, lc.block, 0, st>>>(m, s);
-    else if (lc.min_blocks == 3) k_cell_step_tf<FLUX, VISC, QUAD, 3><<<grid, lc.block, 0, st>>>(m, s);
-    else k_cell_step_tf<FLUX, VISC, QUAD, 2><<<grid, lc.block, 0, st>>>(m, s);
-    return cudaGetLastError();
+    if (lc.min_blocks >= 4) return launch_dependent(k_cell_step_tf<FLUX, VISC, QUAD, 4>, grid, lc.block, st, m, s);
+    if (lc.min_blocks == 3) return launch_dependent(k_cell_step_tf<FLUX, VISC, QUAD, 3>, grid, lc.block, st, m, s);
+    return launch_dependent(k_cell_step_tf<FLUX, VISC, QUAD, 2>, grid, lc.block, st, m, s);
 }
 
 template <int FLUX>

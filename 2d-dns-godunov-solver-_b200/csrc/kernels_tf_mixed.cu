@@ -23,6 +23,8 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
     double *const s_red = reinterpret_cast<double *>(s_buf);
     float4 *const s_prim = reinterpret_cast<float4 *>(s_buf);
     float4 (*const s_flux)[256] = reinterpret_cast<float4 (*)[256]>(s_prim + 256);
+    pdl_trigger();
+    pdl_wait();
     const int par = *s.parity;
     const float4 *__restrict__ pin = s.primf + (int64_t)par * m.Nc;
     float4 *__restrict__ pout = s.primf + (int64_t)(par ^ 1) * m.Nc;
@@ -109,10 +111,9 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
 template <int FLUX, bool VISC, bool QUAD>
 cudaError_t cell_step_tf_m(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
     const int grid = lc.persistent ? lc.grid : (int)m.ntiles;
-    if (lc.min_blocks >= 4) k_cell_step_tf_mixed<FLUX, VISC, QUAD, 4><<<grid, lc.block, 0, st>>>(m, s);
-    else if (lc.min_blocks == 3) k_cell_step_tf_mixed<FLUX, VISC, QUAD, 3><<<grid, lc.block, 0, st>>>(m, s);
-    else k_cell_step_tf_mixed<FLUX, VISC, QUAD, 2><<<grid, lc.block, 0, st>>>(m, s);
-    return cudaGetLastError();
+    if (lc.min_blocks >= 4) return launch_dependent(k_cell_step_tf_mixed<FLUX, VISC, QUAD, 4>, grid, lc.block, st, m, s);
+    if (lc.min_blocks == 3) return launch_dependent(k_cell_step_tf_mixed<FLUX, VISC, QUAD, 3>, grid, lc.block, st, m, s);
+    return launch_dependent(k_cell_step_tf_mixed<FLUX, VISC, QUAD, 2>, grid, lc.block, st, m, s);
 }
 
 template <int FLUX>

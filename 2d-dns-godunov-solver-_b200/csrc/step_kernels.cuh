@@ -21,6 +21,12 @@
 
 namespace gd2d {
 
+// Programmatic dependent launch (launch_dependent): every step kernel lets
+// the next one be scheduled as soon as all its blocks run, and waits for
+// the previous one before it reads or writes any state.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Loads and stores of data a step touches once (per-cell and per-face mesh
 // arrays, the conservative state): marked evict-first, so that the caches
 // keep the gathered node and neighbour data instead.
@@ -490,6 +496,8 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
     double4 *const s_prim = s_mem;
     double4 (*const s_flux)[256] = reinterpret_cast<double4 (*)[256]>(s_mem + 256);
     double *const s_red = reinterpret_cast<double *>(s_mem);
+    pdl_trigger();
+    pdl_wait();
     const int par = *s.parity;
     const double4 *__restrict__ pin = s.prim + (int64_t)par * m.Nc;
     double4 *__restrict__ pout = s.prim + (int64_t)(par ^ 1) * m.Nc;
@@ -579,6 +587,8 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
 template <bool VISC, bool UNIT>
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_node_avg(const DevMesh m, const DevState s, int flip, int zero_prims,
                                                   int64_t n0, int64_t n1) {
+    pdl_trigger();
+    pdl_wait();
     const int par = *s.parity;
     const double4 *__restrict__ src = s.prim + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
     const int W = m.cluster_w;
@@ -653,6 +663,8 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_node_avg(const DevMesh 
 template <bool QUAD>
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_grad1_cells(const DevMesh m, const DevState s) {
     constexpr int NF = QUAD ? 4 : 3;
+    pdl_trigger();
+    pdl_wait();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         // Every per-cell load is issued before any of them is tested, so a
         // cell costs two trips to memory (its own arrays, then the node
@@ -696,6 +708,8 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_grad1_cells(const DevMe
 // gradient fields, calcGradients.jl:3-18).
 static __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_grad1_nodes(const DevMesh m, const DevState s) {
     const int W = m.cluster_w;
+    pdl_trigger();
+    pdl_wait();
     for (int64_t J = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < m.Nn; J += (int64_t)gridDim.x * blockDim.x) {
         double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         int cnt = 0;
