@@ -9,7 +9,9 @@ oracle (same keys, same meaning):
   limiter     "minmod" | "venkat" | "vanleer" | "vanalbada" | "none"
   viscosity   "none" | "reference" | "sutherland" | "constant"
   art_viscosity 0/1, mu_ref, T_ref, Pr, venkat_K, ksi
-  dt_mode     0 fixed ``dt`` | 1 CFL-based ``tau`` (testInviscidFluxesGPUx32.jl:322-324)
+  dt_mode     0 fixed ``dt`` (the reference's solControls.dt, testInviscidFluxesGPUx32.jl:301;
+              the default) | 1 step with the CFL-based ``tau`` the reference only
+              reports (testInviscidFluxesGPUx32.jl:299,324) | 2 local CFL (extension)
   CFL, dt, beta
   init_nodes  0 reference behaviour (node primitives zero in step 1) | 1
   bc          list of {"tag", "kind", rho/u/v/p, Tw}

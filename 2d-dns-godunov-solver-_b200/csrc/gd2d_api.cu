@@ -1129,35 +1129,50 @@ static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, 
                     : launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream);
 }
 
+// Ends the capture opened on the handle's stream in every case (a stream
+// left capturing would refuse all later work) and instantiates the graph.
+// A launch that failed during the capture is reported by its own error,
+// which names the cause, rather than by the capture's generic invalidation;
+// the partial graph is destroyed either way.
+static int end_capture(gd2d_handle *h, cudaError_t launch_err, cudaGraphExec_t *out, const char *what) {
+    cudaGraph_t g = nullptr;
+    const cudaError_t end_err = cudaStreamEndCapture(h->stream, &g);
+    if (launch_err != cudaSuccess || end_err != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        const cudaError_t e = launch_err != cudaSuccess ? launch_err : end_err;
+        return fail(h, GD2D_ERR_CUDA, "%s: %s during %s", what, cudaGetErrorString(e),
+                    launch_err != cudaSuccess ? "a kernel launch of the capture" : "cudaStreamEndCapture");
+    }
+    const cudaError_t e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return fail(h, GD2D_ERR_CUDA, "%s: cudaGraphInstantiate: %s", what, cudaGetErrorString(e));
+    }
+    return GD2D_OK;
+}
+
 static int capture_graph(gd2d_handle *h, int steps, bool timing) {
     drop_graph(h);
     if (timing) {
         h->ev.resize(2 * steps);
         for (auto &e : h->ev) CUDA_TRY(h, cudaEventCreate(&e));
     }
-    cudaGraph_t g;
     CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < steps; ++k) {
-        launch_step_kernels(h, timing ? h->ev[2 * k] : nullptr, timing ? h->ev[2 * k + 1] : nullptr, true);
+    cudaError_t first = cudaSuccess;
+    for (int k = 0; k < steps && first == cudaSuccess; ++k) {
+        first = launch_step_kernels(h, timing ? h->ev[2 * k] : nullptr, timing ? h->ev[2 * k + 1] : nullptr, true);
     }
-    CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&h->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
-    return GD2D_OK;
+    return end_capture(h, first, &h->graph, "step graph");
 }
 
 // A one-step graph (the remainder steps of a propagate call, and single-step
 // calls), timing its cell kernel with the eager event pair.
 static int capture_step_graph(gd2d_handle *h) {
-    cudaGraph_t g;
     CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    launch_step_kernels(h, h->ev_eager[0], h->ev_eager[1], true);
-    CUDA_TRY(h, cudaStreamEndCapture(h->stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&h->graph1, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
-    return GD2D_OK;
+    const cudaError_t first = launch_step_kernels(h, h->ev_eager[0], h->ev_eager[1], true);
+    return end_capture(h, first, &h->graph1, "one-step graph");
 }
 
 int gd2d_propagate(gd2d_handle *h, int32_t nsteps, gd2d_stats *stats_out) {
@@ -1464,7 +1479,14 @@ int gd2d_autotune(gd2d_handle *h, int32_t steps_per_trial, gd2d_launch *chosen) 
         if (e != cudaSuccess) return fail(h, GD2D_ERR_OOM, "autotune snapshot of %zu bytes: %s", total,
                                           cudaGetErrorString(e));
     }
-    CUDA_TRY(h, copy_regions(reg, snap, true, h->stream));
+    {
+        // a failed save must not leak the snapshot buffer
+        cudaError_t e = copy_regions(reg, snap, true, h->stream);
+        if (e != cudaSuccess) {
+            cudaFree(snap);
+            return fail(h, GD2D_ERR_CUDA, "autotune save: %s", cudaGetErrorString(e));
+        }
+    }
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, h->device);
     const LaunchCfg lc0 = h->lc;

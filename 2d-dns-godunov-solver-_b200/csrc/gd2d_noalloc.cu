@@ -130,7 +130,48 @@ k_update_variables_noalloc(const double *__restrict__ unew, double *__restrict__
 }
 
 std::mutex g_addr_mutex;
-void *g_scratch_addr[256] = {nullptr};
+// Device address of the scratch array per device ordinal, with the id of the
+// context it was looked up in: the address is only valid in that context.
+// After cudaDeviceReset (or any other teardown of the primary context) the
+// module is loaded again into a new context, whose id differs, so the
+// address is looked up again rather than reused.
+struct ScratchAddr {
+    void *addr;
+    unsigned long long ctx_id;
+};
+ScratchAddr g_scratch_addr[256] = {};
+
+// The driver's cuCtxGetCurrent / cuCtxGetId, fetched through the runtime (the
+// library links no driver library).  Context ids are unique for the life of
+// the process, unlike context handles, which a new context may reuse.
+typedef int (*PfnCtxGetCurrent)(void **ctx);
+typedef int (*PfnCtxGetId)(void *ctx, unsigned long long *id);
+
+// Id of the calling thread's current context, or 0 when none is current or
+// the driver does not offer context ids.  Called with g_addr_mutex held.
+unsigned long long current_context_id() {
+    static bool looked_up = false;
+    static PfnCtxGetCurrent get_current = nullptr;
+    static PfnCtxGetId get_id = nullptr;
+    if (!looked_up) {
+        looked_up = true;
+        void *f1 = nullptr, *f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<PfnCtxGetCurrent>(f1);
+            get_id = reinterpret_cast<PfnCtxGetId>(f2);
+        }
+        (void)cudaGetLastError();
+    }
+    if (!get_current || !get_id) return 0;
+    void *ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_current(&ctx) != 0 || !ctx) return 0;
+    if (get_id(ctx, &id) != 0) return 0;
+    return id;
+}
 
 int noalloc_fail(int code, const char *msg) {
     gd2d::set_handleless_error(msg);
@@ -157,10 +198,13 @@ extern "C" int gd2d_update_variables_noalloc(const double *d_unew, double *d_uol
         return noalloc_fail(GD2D_ERR_CUDA, "gd2d_update_variables_noalloc: no current CUDA device");
     double *scratch = nullptr;
     {
-        // Once per device, with that device current: the device address of
-        // the scratch symbol (the host-side name is only a stand-in).
+        // Once per device (per context of that device), with that device
+        // current: the device address of the scratch symbol (the host-side
+        // name is only a stand-in, never a device address).
         std::lock_guard<std::mutex> lock(g_addr_mutex);
-        if (!g_scratch_addr[dev]) {
+        ScratchAddr &sa = g_scratch_addr[dev];
+        const unsigned long long ctx = current_context_id();
+        if (!sa.addr || ctx == 0 || ctx != sa.ctx_id) {
             void *p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) {
@@ -169,9 +213,11 @@ extern "C" int gd2d_update_variables_noalloc(const double *d_unew, double *d_uol
                          cudaGetErrorString(e));
                 return noalloc_fail(GD2D_ERR_CUDA, buf);
             }
-            g_scratch_addr[dev] = p;
+            sa.addr = p;
+            // the lookup made the device's context current if it was not yet
+            sa.ctx_id = current_context_id();
         }
-        scratch = static_cast<double *>(g_scratch_addr[dev]);
+        scratch = static_cast<double *>(sa.addr);
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int64_t ntiles = (n_cells + kNoAllocTile - 1) / kNoAllocTile;

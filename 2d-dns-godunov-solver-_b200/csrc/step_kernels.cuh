@@ -139,7 +139,9 @@ __device__ __forceinline__ Part warp_reduce_records(const double *recs, int64_t 
 // Per-case finalization by the warp that completed the case's last tile
 // group: reduce the group records in a fixed order, publish the step
 // statistics and advance time (flowTime += dt, testInviscidFluxesGPUx32.jl:401)
-// and the next dt (tau at :322-324, or the local-CFL extension).
+// and the next dt: the fixed solControls.dt the reference steps with, or
+// opt-in, the tau it reports (testInviscidFluxesGPUx32.jl:299,324) or the
+// local-CFL extension.
 static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c, bool is_init) {
     const DevCase &P = m.cases[c];
     const Part acc = warp_reduce_records(s.gpart, P.group_begin, P.group_end);

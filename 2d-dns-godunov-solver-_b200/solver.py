@@ -48,6 +48,12 @@ def make_params(cfg: Dict) -> N.Params:
     p.RGAS, p.Gamma = th["RGAS"], th["Gamma"]
     p.Cp, p.mu, p.kGas = th.get("Cp", 1000.0), th.get("mu", 0.0), th.get("kGas", 0.0)
     p.CFL = cfg.get("CFL", 0.5)
+    # the reference steps with the fixed solControls.dt
+    # (testInviscidFluxesGPUx32.jl:324 only reports the CFL-based tau);
+    # the CFL-driven modes are opt-in
+    p.dt_mode = int(cfg.get("dt_mode", 0))
+    if p.dt_mode == 0 and not cfg.get("dt", 0.0) > 0.0:
+        raise ValueError("dt_mode 0 (fixed time step, the reference's solControls.dt) needs a positive 'dt'")
     p.dt = cfg.get("dt", 0.0)
     p.beta = cfg.get("beta", 1.0)
     p.ksi = cfg.get("ksi", 1.0e-12)
@@ -66,7 +72,6 @@ def make_params(cfg: Dict) -> N.Params:
     p.limiter = N.LIMITER[cfg.get("limiter", "minmod")]
     p.viscosity = N.VISC[cfg.get("viscosity", "none")]
     p.art_viscosity = int(cfg.get("art_viscosity", 0))
-    p.dt_mode = int(cfg.get("dt_mode", 1))
     p.init_nodes = int(cfg.get("init_nodes", 0))
     bcs = cfg.get("bc", [])
     if len(bcs) > N.GD2D_MAX_BC:

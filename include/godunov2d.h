@@ -54,8 +54,12 @@ enum gd2d_bc_kind { GD2D_BC_INFLOW = 1, GD2D_BC_OUTFLOW = 2, GD2D_BC_SLIP_WALL =
  * air conductivity); SUTHERLAND / CONSTANT are extensions. */
 enum gd2d_viscosity { GD2D_VISC_NONE = 0, GD2D_VISC_REFERENCE = 1, GD2D_VISC_SUTHERLAND = 2,
                       GD2D_VISC_CONSTANT = 3 };
-/* Time step: FIXED = solControls.dt; REFERENCE_TAU = CFL*max(HX)/max(VMAX)
- * (testInviscidFluxesGPUx32.jl:322-324); LOCAL_CFL = CFL*min(2A/P/VMAX). */
+/* Time step: FIXED = solControls.dt, what the reference steps with
+ * (testInviscidFluxesGPUx32.jl:301, flowTime += dt at :401).
+ * REFERENCE_TAU = step with tau = CFL*max(HX)/max(VMAX), which the reference
+ * computes and reports every step (testInviscidFluxesGPUx32.jl:299,324) but
+ * does not step with.  LOCAL_CFL = CFL*min(2A/P/VMAX) (extension).  tau is
+ * reported in gd2d_stats under every mode. */
 enum gd2d_dt_mode { GD2D_DT_FIXED = 0, GD2D_DT_REFERENCE_TAU = 1, GD2D_DT_LOCAL_CFL = 2 };
 enum gd2d_precision { GD2D_PREC_F64 = 0, GD2D_PREC_MIXED = 1 };
 enum gd2d_order { GD2D_ORDER_NATURAL = 0, GD2D_ORDER_HILBERT = 1, GD2D_ORDER_RCM = 2 };
@@ -234,7 +238,8 @@ int gd2d_destroy(gd2d_handle *h);
  * doubles = sum of (Unew-Uold)^2 per variable, max VMAX, non-finite flag.
  * The only scratch is a fixed 4 MiB array inside the library (one per GPU,
  * held until exit), so n_cells is limited to 16,777,216 (larger: GD2D_ERR_ARG).
- * The first call on a device looks that array up and should come before any
+ * The first call on a device looks that array up (again after the device's
+ * context is recreated, e.g. by cudaDeviceReset) and should come before any
  * stream capture; calls that overlap on the GPU share the array and race.
  * Runs on `stream` (NULL: the legacy default stream). */
 int gd2d_update_variables_noalloc(const double *d_unew, double *d_uold, double *d_prims, int64_t n_cells,

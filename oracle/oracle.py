@@ -154,7 +154,7 @@ def make_params(cfg) -> OrcParams:
     p.limiter = LIMITER[cfg.get("limiter", "minmod")]
     p.viscosity = VISC[cfg.get("viscosity", "none")]
     p.art_viscosity = int(cfg.get("art_viscosity", 0))
-    p.dt_mode = int(cfg.get("dt_mode", 1))
+    p.dt_mode = int(cfg.get("dt_mode", 0))
     p.init_nodes = int(cfg.get("init_nodes", 0))
     p.nthreads = int(cfg.get("nthreads", os.cpu_count() or 1))
     bcs = cfg.get("bc", [])

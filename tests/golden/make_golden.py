@@ -15,7 +15,8 @@ the GPU tests can run the reference's own mesh without the reference
 checkout, and records a digest of every dataset in
 tests/golden/oblique_shock_mesh.json.
 
-Run: python tests/golden/make_golden.py
+Run: GD2D_REFERENCE_DIR=<reference checkout> python tests/golden/make_golden.py
+(without GD2D_REFERENCE_DIR only the Riemann-pair file is written).
 """
 import json
 import os
@@ -120,7 +121,9 @@ def main():
     convert_reference_mesh()
 
 
-def convert_reference_mesh(src="/root/reference/oblickShock2dl00F1n.h5"):
+def convert_reference_mesh(src=None):
+    """Convert the reference repository's mesh file, found in the checkout
+    named by GD2D_REFERENCE_DIR (skipped when that is unset)."""
     import hashlib
     import sys
     import numpy as np
@@ -131,6 +134,12 @@ def convert_reference_mesh(src="/root/reference/oblickShock2dl00F1n.h5"):
     pkg = graft.load_package()
     from importlib import import_module
     h5 = import_module(graft.PKG_NAME + ".hdf5mesh")
+    if src is None:
+        ref_dir = os.environ.get("GD2D_REFERENCE_DIR")
+        if not ref_dir:
+            print("GD2D_REFERENCE_DIR not set; reference mesh conversion skipped")
+            return
+        src = os.path.join(ref_dir, "oblickShock2dl00F1n.h5")
     if not os.path.exists(src):
         print("reference mesh not found; skipped", src)
         return

@@ -45,11 +45,24 @@ def compare_state(s, o, icase=0):
 
 
 def compare_stats(gh, oh, tol):
+    """Per-step statistics against the oracle's.  Maxima and minima (VMAX,
+    tau = CFL max(HX) / max(VMAX), the density extremes) are order-free and
+    must be equal; sums (residuals, conserved totals, kinetic energy) are
+    reduced in a different order on the GPU, so they are compared to 1e-12
+    relative (residuals 1e-10: they are differences of nearly equal states),
+    with the momentum totals scaled by the momentum magnitude since one of
+    them may be zero."""
     for a, b in zip(gh, oh):
         assert a["dt"] == pytest.approx(b["dt"], rel=tol, abs=0)
         assert a["flowTime"] == pytest.approx(b["flowTime"], rel=tol, abs=1e-300)
+        assert a["tau"] == b["tau"] and a["velmax"] == b["velmax"]
         for v in range(4):
             assert a["residual"][v] == pytest.approx(b["residual"][v], rel=1e-10, abs=1e-300)
+        mom = float(np.hypot(b["totals"][1], b["totals"][2]))
+        scale = [abs(b["totals"][0]), mom, mom, abs(b["totals"][3])]
+        for v in range(4):
+            assert abs(a["totals"][v] - b["totals"][v]) <= 1e-12 * max(scale[v], 1e-300), (v, a["totals"], b["totals"])
+        assert a["Ek"] == pytest.approx(b["Ek"], rel=1e-12, abs=1e-300)
         assert a["rhoMin"] == b["rhoMin"] and a["rhoMax"] == b["rhoMax"]
         assert a["nonfinite"] == 0 and b["nonfinite"] == 0
 
@@ -67,6 +80,22 @@ def test_square_inviscid_step_and_100(pkg, orc):
     eU, eP, eN, bit = compare_state(s, o)
     assert max(eU, eP, eN) <= TOL_100, (eU, eP, eN)
     compare_stats(gh, oh, 1e-12)
+
+
+def test_reference_tau_time_step(pkg, orc):
+    """dt_mode 1 steps with the tau the reference reports every step,
+    tau = CFL max(HX) / max(max(VMAX), 1e-6) (testInviscidFluxesGPUx32.jl:299,324),
+    at CFL 0.2 where the jittered square stays admissible.  dt must equal the
+    oracle's bit for bit in every one of 100 steps, and the state must be
+    bit-identical after them."""
+    mesh, cfg, prims = pkg.cases.square_inviscid(101)
+    cfg = dict(cfg, dt_mode=1, CFL=0.2)
+    s, o, gh, oh = run_pair(pkg, orc, mesh, cfg, prims, 100)
+    for a, b in zip(gh, oh):
+        assert a["dt"] == b["dt"] == b["tau"], (a["dt"], b["dt"], b["tau"])
+    compare_stats(gh, oh, 0.0)
+    eU, eP, eN, bit = compare_state(s, o)
+    assert bit and max(eU, eP, eN) == 0.0, (eU, eP, eN)
 
 
 @pytest.mark.parametrize("order", ["natural", "hilbert", "rcm"])

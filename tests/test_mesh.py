@@ -89,9 +89,12 @@ def test_hdf5_reader_matches_recorded_digests(pkg):
     import hashlib
     import json
     import os
-    src = "/root/reference/oblickShock2dl00F1n.h5"
+    ref_dir = os.environ.get("GD2D_REFERENCE_DIR")
+    if not ref_dir:
+        pytest.skip("GD2D_REFERENCE_DIR (a checkout of the reference repository) is not set")
+    src = os.path.join(ref_dir, "oblickShock2dl00F1n.h5")
     if not os.path.exists(src):
-        pytest.skip("reference checkout not present")
+        pytest.skip("reference mesh file not present in GD2D_REFERENCE_DIR")
     from importlib import import_module
     h5 = import_module(pkg.__name__ + ".hdf5mesh")
     ds = h5.read_datasets(src)
