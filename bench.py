@@ -233,6 +233,39 @@ def cpu_reference(pkg, items, steps, warmup, budget_s=25.0, single_thread_s=8.0)
             "repeats": [round(r, 4) for r in rates], "single_thread_value": single, "host": cpu_model()}
 
 
+def parity_block(pkg, items, s, steps=100):
+    """The FP64 GPU step against the CPU oracle on the full workload (case 0),
+    both from the same initial state: per-variable max|gpu - oracle| / max|oracle|
+    of the conservative state after step 1 and after `steps` steps, and
+    whether the states are equal bit for bit.  Tolerances: 1e-12 per step,
+    1e-10 after 100 steps."""
+    from oracle import oracle as orc
+    orc.build()
+    mesh, cfg, prims = items[0]
+    nthreads = os.cpu_count() or 1
+    o = orc.Oracle(mesh, cfg, nthreads=nthreads)
+    o.init_fields(*prims)
+    s.createFields2d(0, *prims)
+    out = {"cells": mesh.nCells, "oracle_threads": nthreads, "vars": ["rho", "rho_u", "rho_v", "E"],
+           "tolerance": {"1": 1e-12, str(steps): 1e-10}}
+    t0 = time.perf_counter()
+    done = 0
+    for k in (1, steps):
+        s.propagate2d(k - done)
+        for _ in range(k - done):
+            o.step()
+        done = k
+        g = s.get_state(0)["Ucons"]
+        r = o.field("Uold")
+        scale = np.maximum(np.abs(r).max(axis=0), 1e-300)
+        err = (np.abs(g - r).max(axis=0) / scale)
+        out["after_%d" % k] = {"max_rel_err": [float(x) for x in err], "bit_equal": bool(np.array_equal(g, r))}
+    out["seconds"] = round(time.perf_counter() - t0, 1)
+    out["pass"] = bool(max(out["after_1"]["max_rel_err"]) <= 1e-12 and
+                       max(out["after_%d" % steps]["max_rel_err"]) <= 1e-10)
+    return out
+
+
 def mixed_variant(pkg, items, s64, args, peak):
     """The same workload on the mixed-precision path: device-timed
     throughput, and the error after --error-steps steps against the FP64 path
@@ -302,6 +335,8 @@ def main():
                     help="let gd2d_autotune pick the launch shape before the warm-up")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
+    ap.add_argument("--no-parity", action="store_true", help="skip the FP64 GPU-vs-oracle parity check")
+    ap.add_argument("--parity-steps", type=int, default=100, help="steps of the parity check")
     ap.add_argument("--error-steps", type=int, default=1000,
                     help="steps of the mixed-vs-FP64 error measurement")
     args = ap.parse_args()
@@ -422,6 +457,9 @@ def main():
                          "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak},
             "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches), "clocks": clocks}
+    if args.config in ("cylinder", "square") and args.precision == "f64" and rank == 0 and world == 1 \
+            and not args.no_parity:
+        line["parity"] = parity_block(pkg, items, s, args.parity_steps)
     if args.config in ("cylinder", "square") and args.precision == "f64" and not args.no_mixed:
         line["mixed"] = mixed_variant(pkg, items, s, args, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

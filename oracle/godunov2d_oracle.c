@@ -732,6 +732,14 @@ static void gg_gradient(orc_state *s, const double *field, double *gx, double *g
     parallel(s, s->cellsThreads, gg_range, &c);
 }
 
+/* The same gradient of an arbitrary cell field (nCells values), as the
+ * reference's operator driver calls it (testDiffOperatorsGrads.jl:303,
+ * testDiffOperatorsLaplace.jl:98-105): node values are the unweighted cluster
+ * means of the field, gradX pairs with -ny and gradY with -nx. */
+void orc_green_gauss_gradient(orc_state *s, const double *field, double *gx, double *gy) {
+    gg_gradient(s, field, gx, gy);
+}
+
 /* nodesGradientReconstructionFastPerThread22, calcGrad.jl:3-96 (node field,
  * -nx for x); used for the velocity divergence of the artificial viscosity. */
 static void node_grad_cell(const orc_state *s, int64_t C, const double *nodeField, double *gx, double *gy) {

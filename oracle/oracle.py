@@ -88,6 +88,7 @@ def lib():
         L.orc_update_variables.argtypes = [C.c_void_p, C.POINTER(OrcStats)]
         L.orc_cells2nodes.argtypes = [C.c_void_p]
         L.orc_calc_diff_term.argtypes = [C.c_void_p]
+        L.orc_green_gauss_gradient.argtypes = [C.c_void_p, dp, dp, dp]
         L.orc_field.restype = dp
         L.orc_field.argtypes = [C.c_void_p, C.c_int32]
         L.orc_flow_time.restype = C.c_double
@@ -223,6 +224,19 @@ class Oracle:
 
     def calc_diff_term(self):
         lib().orc_calc_diff_term(self.h)
+
+    def green_gauss_gradient(self, field):
+        """calcScalarFieldGreenGaussNodesBasedGradient (calcGradients.jl:36-139)
+        of a cell field: (gradX, gradY), gradX paired with -ny as in the
+        reference, so gradX approximates d/dy and gradY d/dx for the mesh's
+        inward unit normals."""
+        f = np.ascontiguousarray(field, dtype=np.float64)
+        if f.shape != (self.mesh.nCells,):
+            raise ValueError("field size does not match the mesh")
+        gx = np.zeros_like(f)
+        gy = np.zeros_like(f)
+        lib().orc_green_gauss_gradient(self.h, _dptr(f), _dptr(gx), _dptr(gy))
+        return gx, gy
 
     def field(self, name):
         n = self.mesh.nNodes if name in ("rhoN", "uxN", "uyN", "pN", "UN") else self.mesh.nCells

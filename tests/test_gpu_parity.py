@@ -150,6 +150,32 @@ def test_cylinder_sutherland_artvisc_venkat(pkg, orc):
     compare_stats(gh, oh, 1e-12)
 
 
+@pytest.mark.parametrize("loop", ["tile", "cell"])
+def test_cylinder_513_bit_exact_100_steps(pkg, orc, loop):
+    """The viscous supersonic cylinder on a 513^2 node grid (522,984 cells;
+    M 3.5, Re_D 1e4, Sutherland + artificial viscosity, Venkatakrishnan,
+    no-slip isothermal wall, local CFL 0.4): the FP64 GPU state equals the
+    oracle's bit for bit after step 1 and after step 100, with every step's
+    statistics matched (tolerances of compare_stats)."""
+    import os
+    mesh, cfg, prims = pkg.cases.cylinder_case(513)
+    cfg = dict(cfg, dt_mode=2)
+    s = pkg.setupSolver(mesh, cfg, loop=loop)
+    s.createFields2d(0, *prims)
+    o = orc.Oracle(mesh, cfg, nthreads=os.cpu_count() or 4)
+    o.init_fields(*prims)
+    gh, oh = [s.propagate2d(1)[0]], [o.step()]
+    eU, eP, eN, bit = compare_state(s, o)
+    assert bit and max(eU, eP, eN) == 0.0, ("step 1", eU, eP, eN)
+    for _ in range(99):
+        gh.append(s.propagate2d(1)[0])
+        oh.append(o.step())
+    eU, eP, eN, bit = compare_state(s, o)
+    assert bit and max(eU, eP, eN) == 0.0, ("step 100", eU, eP, eN)
+    compare_stats(gh, oh, 0.0)
+    s.close()
+
+
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
 def test_edge_pairs_listed_end_first(pkg, orc, precision):
     """cells2nodes may list an edge's node pair in either order: the viscous
