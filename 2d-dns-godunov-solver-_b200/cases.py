@@ -83,7 +83,8 @@ def cylinder_case(n_nodes: int = 1025, mach: float = 3.5, re_d: float = 1.0e4, r
            "densityConstrained": 1, "minDensityConstrained": 0.01, "maxDensityConstrained": 10.0,
            "bc": [{"tag": -1, "kind": "inflow", "rho": CYL_RHO, "u": u_inf, "v": 0.0, "p": CYL_P},
                   {"tag": -2, "kind": "outflow"},
-                  {"tag": -4, "kind": "noslip_isothermal", "Tw": T_inf}]}
+                  {"tag": -4, "kind": "noslip_isothermal", "Tw": T_inf}],
+           "case_info": {"mach": mach, "re_d": re_d, "radius": radius, "nodes_per_side": n_nodes}}
     nc = mesh.nCells
     prims = (np.full(nc, CYL_RHO), np.full(nc, u_inf), np.zeros(nc), np.full(nc, CYL_P))
     return mesh, cfg, prims
@@ -101,7 +102,7 @@ def tgv_case(n_nodes: int, mach: float, re: float, flux: str = "ausm", limiter: 
     mu = 1.0 * U0 * 1.0 / re
     cfg = {"thermo": th, "flux": flux, "limiter": limiter, "viscosity": "constant", "art_viscosity": 0,
            "mu_ref": mu, "T_ref": 1.0, "Pr": 0.72, "dt_mode": 2, "CFL": cfl, "beta": 1.0, "ksi": 1.0e-12,
-           "init_nodes": 0, "bc": []}
+           "init_nodes": 0, "bc": [], "case_info": {"mach": mach, "re": re, "nodes_per_side": n_nodes}}
     x, y = mesh.cell_mid_points[:, 0], mesh.cell_mid_points[:, 1]
     u = U0 * np.sin(x) * np.cos(y)
     v = -U0 * np.cos(x) * np.sin(y)

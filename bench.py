@@ -314,6 +314,117 @@ def mixed_variant(pkg, items, s64, args, peak):
                               "vars": ["rho", "rho_u", "rho_v", "E"], "totals_drift_rel": drift}}
 
 
+def batched_mixed(pkg, items, s64, args, peak, kind):
+    """Configs 4 and 5: every case of the batch on the mixed-precision path in
+    one handle (one launch per kernel per step for all cases), launch shapes
+    picked by gd2d_autotune starting from a 100-step CUDA graph; device-timed
+    aggregate throughput and roofline, then a per-case error after
+    `--error-steps` steps against the FP64 path from the same initial states
+    (the FP64 path is bit-identical to the CPU oracle in the parity tests, so
+    it stands in for the oracle at these sizes).  TGV: the relative error of
+    the kinetic energy Ek(t) and of its decay E0 - Ek(t); cylinders: the
+    relative L2 error of the density."""
+    meshes = [m for m, _, _ in items]
+    cfgs = [c for _, c, _ in items]
+    cells = sum(m.nCells for m in meshes)
+    sm = pkg.solver.Solver(meshes, cfgs, pkg.solver.make_launch(precision="mixed", order=args.order, loop=args.loop,
+                                                                device=args.device, graph_steps=100))
+    for i, (_, _, p) in enumerate(items):
+        sm.createFields2d(i, *p)
+    tuned = sm.autotune(64)
+    sm.propagate2d(args.gpu_warmup)
+    sm.propagate2d(args.steps)
+    tot, cell_ms, launches = sm.last_timing()
+    value = cells * args.steps / (tot / 1e3) / 1e6
+    alg = ALG_BYTES[("mixed", cfgs[0].get("viscosity", "none") != "none")]
+    n_err = args.error_steps
+    for i, (_, _, p) in enumerate(items):
+        sm.createFields2d(i, *p)
+        s64.createFields2d(i, *p)
+    sm.propagate2d(n_err)
+    s64.propagate2d(n_err)
+    per_case = []
+    for i, (m, c, p) in enumerate(items):
+        rec = dict({"case": i, "cells": m.nCells}, **c.get("case_info", {}))
+        if kind == "tgv":
+            rho, u, v, _ = p
+            e0 = float((0.5 * rho * (u * u + v * v) * m.cell_areas).sum())
+            ekm, ek64 = sm.history(i, 1)[-1]["Ek"], s64.history(i, 1)[-1]["Ek"]
+            rec.update({"ek_over_e0_fp64": ek64 / e0,
+                        "ek_rel_err": abs(ekm - ek64) / ek64,
+                        "decay_rel_err": abs((e0 - ekm) - (e0 - ek64)) / max(e0 - ek64, 1e-300)})
+        else:
+            rm = sm.get_state(i)["Ucons"][:, 0]
+            r64 = s64.get_state(i)["Ucons"][:, 0]
+            rec["rho_l2_rel_err"] = float(np.sqrt(((rm - r64) ** 2).sum() / (r64 ** 2).sum()))
+            rec["rho_linf_rel_err"] = float(np.abs(rm - r64).max() / np.abs(r64).max())
+        per_case.append(rec)
+    sm.close()
+    key = "decay_rel_err" if kind == "tgv" else "rho_l2_rel_err"
+    achieved = alg * cells / (cell_ms / 1e3) / 1e9 if cell_ms else None
+    return {"value": value, "unit": "Mcell-steps/s", "cells": cells, "ms_per_step": tot / args.steps,
+            "cell_kernel_ms": cell_ms, "gpu_launches": int(launches), "autotuned_launch": tuned,
+            "roofline": {"achieved": achieved, "peak": peak, "frac": achieved / peak if achieved else None,
+                         "alg_bytes_per_cell": alg,
+                         "step_achieved_gbs": alg * cells / (tot / args.steps / 1e3) / 1e9},
+            "error_vs_fp64": {"steps": n_err, "max_" + key: max(r[key] for r in per_case), "per_case": per_case}}
+
+
+def roe_from_developed_flow(pkg, items, args):
+    """Config 3 with the Roe flux on the cylinder.  An impulsive start takes
+    the Roe flux out of the admissible set at the wall, so the comparison
+    starts from a developed flow: `--roe-restart` FP64 AUSM+ steps from the
+    freestream, then that conservative state and flowTime restart an FP64 and
+    a mixed-precision handle with the Roe flux (gd2d_set_conservative), which
+    run `--error-steps` steps each.  Reports the mixed-vs-FP64 errors as
+    mixed_variant does, or where the FP64 Roe run left the admissible set."""
+    mesh, cfg, prims = items[0]
+    mk = pkg.solver.make_launch
+    base = pkg.solver.Solver([mesh], [dict(cfg, flux="ausm")], mk(precision="f64", order=args.order, loop=args.loop,
+                                                                   device=args.device))
+    base.createFields2d(0, *prims)
+    base.propagate2d(args.roe_restart)
+    U0 = base.get_state(0)["Ucons"]
+    t0 = base.flow_time(0)
+    base.close()
+    roe = dict(cfg, flux="roe")
+    out = {"restart_steps_ausm": args.roe_restart, "restart_flow_time": t0, "steps": args.error_steps}
+    runs = {}
+    for prec in ("f64", "mixed"):
+        h = pkg.solver.Solver([mesh], [roe], mk(precision=prec, order=args.order, loop=args.loop, device=args.device))
+        h.set_conservative(0, U0, t0)
+        done, failed = 0, None
+        while done < args.error_steps:
+            n = min(500, args.error_steps - done)
+            try:
+                h.propagate2d(n)
+            except pkg._native.NativeError as e:
+                failed = {"after_steps": done + n, "error": str(e)}
+                break
+            done += n
+        runs[prec] = (h, failed)
+        out[prec + "_failed"] = failed
+    if runs["f64"][1] is None and runs["mixed"][1] is None:
+        Um = runs["mixed"][0].get_state(0)["Ucons"]
+        U64 = runs["f64"][0].get_state(0)["Ucons"]
+        d = Um - U64
+        mom = np.sqrt(U64[:, 1] ** 2 + U64[:, 2] ** 2)
+        n2 = np.sqrt((U64 ** 2).sum(axis=0))
+        n2[1] = n2[2] = np.sqrt((mom ** 2).sum())
+        ninf = np.abs(U64).max(axis=0)
+        ninf[1] = ninf[2] = mom.max()
+        out["l2_rel"] = [float(x) for x in np.sqrt((d ** 2).sum(axis=0)) / np.maximum(n2, 1e-300)]
+        out["linf_rel"] = [float(x) for x in np.abs(d).max(axis=0) / np.maximum(ninf, 1e-300)]
+        hm, h64 = runs["mixed"][0].history(0), runs["f64"][0].history(0)
+        tm0, t640 = hm[0]["totals"], h64[0]["totals"]
+        tscale = [abs(t640[0]), math.hypot(t640[1], t640[2]), math.hypot(t640[1], t640[2]), abs(t640[3])]
+        out["totals_drift_rel"] = [abs((hm[-1]["totals"][v] - tm0[v]) - (h64[-1]["totals"][v] - t640[v]))
+                                   / max(tscale[v], 1e-300) for v in range(4)]
+    for h, _ in runs.values():
+        h.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -337,9 +448,13 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision comparison")
     ap.add_argument("--no-parity", action="store_true", help="skip the FP64 GPU-vs-oracle parity check")
     ap.add_argument("--parity-steps", type=int, default=100, help="steps of the parity check")
-    ap.add_argument("--error-steps", type=int, default=1000,
-                    help="steps of the mixed-vs-FP64 error measurement")
+    ap.add_argument("--roe-restart", type=int, default=0,
+                    help="cylinder: compare Roe mixed vs FP64 from the state after this many AUSM+ steps")
+    ap.add_argument("--error-steps", type=int, default=0,
+                    help="steps of the mixed-vs-FP64 error measurement (0: 1000; cyl_batch 2000)")
     args = ap.parse_args()
+    if args.error_steps <= 0:
+        args.error_steps = 2000 if args.config == "cyl_batch" else 1000
     # at least 3 warm-up steps, and at least one CUDA graph's worth
     args.warmup = max(args.warmup, 3)
     # the GPU arm warms up at least one CUDA graph's worth of steps
@@ -423,18 +538,37 @@ def main():
     dp = C.POINTER(C.c_double)
     dist_barrier(dist)
     e2e_steps = args.steps
-    t0 = time.perf_counter()
+    tick = time.perf_counter
+    call_s, call_dev_ms = [], []
+    tdev = C.c_double()
+    t0 = tick()
     for i, hp in enumerate(host_prims):
         N.check(L.gd2d_set_state(s.h, i, *[a.ctypes.data_as(dp) for a in hp]), s.h)
+    t1 = tick()
     for _ in range(e2e_steps):
+        ta = tick()
         N.check(L.gd2d_propagate(s.h, 1, st), s.h)
+        call_s.append(tick() - ta)
+        L.gd2d_last_timing(s.h, C.byref(tdev), None, None)
+        call_dev_ms.append(tdev.value)
+    t2 = tick()
     for i, u in enumerate(ucons):
         N.check(L.gd2d_get_state(s.h, i, u.ctypes.data_as(dp), None, None), s.h)
-    e2e_s = time.perf_counter() - t0
+    t3 = tick()
+    e2e_s = t3 - t0
     e2e_s = dist_max(dist, e2e_s)
     e2e_val = job_cells * e2e_steps / e2e_s / 1e6
     h2d = 4 * 8 * cells / e2e_steps
     d2h = C.sizeof(N.Stats) * len(meshes) + 4 * 8 * cells / e2e_steps
+    # where the end-to-end time goes: host clock around each call, and the
+    # device time (CUDA events on the stream) of each one-step propagate
+    e2e_breakdown = {"set_state_ms": (t1 - t0) * 1e3, "get_state_ms": (t3 - t2) * 1e3,
+                     "propagate_calls_ms": (t2 - t1) * 1e3,
+                     "propagate_call_median_ms": statistics.median(call_s) * 1e3,
+                     "propagate_call_device_median_ms": statistics.median(call_dev_ms),
+                     "propagate_call_host_overhead_median_us":
+                         (statistics.median(call_s) * 1e3 - statistics.median(call_dev_ms)) * 1e3,
+                     "timed_region_device_ms_per_step": None}
 
     peak, peak_kind = load_peaks()
     alg = ALG_BYTES[(args.precision, viscous)]
@@ -455,13 +589,18 @@ def main():
                                    + " (fused reconstruction+flux+viscous+update)",
                          "alg_bytes_per_cell": alg, "cell_kernel_ms": cell_ms, "peak_kind": peak_kind,
                          "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak},
-            "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps, "breakdown": dict(e2e_breakdown, timed_region_device_ms_per_step=ms_per_step)},
             "gpu_launches": int(launches), "clocks": clocks}
     if args.config in ("cylinder", "square") and args.precision == "f64" and rank == 0 and world == 1 \
             and not args.no_parity:
         line["parity"] = parity_block(pkg, items, s, args.parity_steps)
     if args.config in ("cylinder", "square") and args.precision == "f64" and not args.no_mixed:
         line["mixed"] = mixed_variant(pkg, items, s, args, peak)
+    if args.config in ("tgv_batch", "cyl_batch") and args.precision == "f64" and not args.no_mixed:
+        line["mixed"] = batched_mixed(pkg, items, s, args, peak, "tgv" if args.config == "tgv_batch" else "cyl")
+    if args.config == "cylinder" and args.roe_restart > 0 and world == 1:
+        line["roe_from_developed_flow"] = roe_from_developed_flow(pkg, items, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(pkg, items, args.steps, args.warmup)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "repeats",
