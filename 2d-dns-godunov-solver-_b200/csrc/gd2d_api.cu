@@ -641,7 +641,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     // cells of the same kind and exactly one slot of each facing the other
     std::vector<int64_t> tf_off;
     std::vector<int4> tf_rec;
-    std::vector<int2> tf_q;
+    std::vector<int2> tf_q, tf_e;
     std::vector<double> tf_nx, tf_ny, tf_len;
     if (h->loop == GD2D_LOOP_TILE_FACES) {
         std::vector<char> case_pairs(n_cases, 0);
@@ -668,6 +668,12 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
             if (is_quad_cell(lo) && (code_k(dn2[hi], khi) != code_k(up2[lo], klo) ||
                                      code_k(up2[hi], khi) != code_k(dn2[lo], klo)))
                 return false;
+            // the viscous edge terms are negated for the other cell too: the
+            // two slots name the same pair of edge nodes (in either order)
+            if (h->visc) {
+                const int2 el = c2n[ol], eh = c2n[oh];
+                if (!((el.x == eh.x && el.y == eh.y) || (el.x == eh.y && el.y == eh.x))) return false;
+            }
             return true;
         };
         tf_off.assign(ntiles + 1, 0);
@@ -698,6 +704,7 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
                                                code_k(up[g], k)));
                     if (h->quads) tf_q.push_back(make_int2(code_k(dn2[g], k), code_k(up2[g], k)));
                     const size_t o = (size_t)k * Nc + g;
+                    if (h->visc) tf_e.push_back(c2n[o]);
                     tf_nx.push_back(gnx[o]);
                     tf_ny.push_back(gny[o]);
                     tf_len.push_back(glen[o]);
@@ -807,6 +814,11 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         ALLOC(d_tfo, tf_off.size()); UPLOAD(d_tfo, tf_off);
         ALLOC(d_tfr, tf_rec.size()); UPLOAD(d_tfr, tf_rec);
         if (h->quads) { ALLOC(d_tfq, tf_q.size()); UPLOAD(d_tfq, tf_q); }
+        if (h->visc) {
+            int2 *d_tfe;
+            ALLOC(d_tfe, tf_e.size()); UPLOAD(d_tfe, tf_e);
+            m.tf_e = d_tfe;
+        }
         if (!h->mixed) {
             ALLOC(d_tnx, tf_nx.size()); UPLOAD(d_tnx, tf_nx);
             ALLOC(d_tny, tf_ny.size()); UPLOAD(d_tny, tf_ny);

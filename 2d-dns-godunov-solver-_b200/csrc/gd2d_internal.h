@@ -108,6 +108,7 @@ struct DevMesh {
     const int64_t *tf_off;               // [ntiles + 1]
     const int4 *tf_rec;
     const int2 *tf_q;
+    const int2 *tf_e;                    // (viscous) edge node pair of slot (la, ka)
     const double *tf_nx, *tf_ny, *tf_len;
     const float *tf_nxf, *tf_nyf, *tf_lenf;
 };

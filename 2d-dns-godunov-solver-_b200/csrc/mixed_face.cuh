@@ -106,6 +106,58 @@ __device__ __forceinline__ float4 avg4(const float4 &a, const float4 &b) {
     return make_float4(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z), 0.5f * (a.w + b.w));
 }
 
+// Transport model of the diffusion source (calcDiffTerm.jl:105-113; the
+// Sutherland / constant extensions with artificial viscosity per
+// calcArtViscosity.jl:46-75) applied to the cell's Laplacians `lap` (of
+// rho u, rho v, E in the reference form; of u, v, |u|^2/2 + (gamma/Pr) e
+// otherwise) and, for the artificial viscosity, its velocity divergence.
+__device__ __forceinline__ void visc_source_f(const DevCase &P, const float4 &me, const float *lap, float divU,
+                                              float HX, float *diff) {
+    const float T = me.w / me.x / (float)P.R;
+    diff[0] = 0.f;
+    if (P.visc_model == VISC_REFERENCE) {
+        const float mu = (float)P.mu_ref;
+        diff[1] = mu * lap[0];
+        diff[2] = mu * lap[1];
+        diff[3] = mu * (float)air_conductivity((double)T) * lap[2];
+    } else {
+        const float mu = (P.visc_model == VISC_SUTHERLAND)
+                             ? (float)P.mu_ref * (sutherland(T) / (float)P.suth_ref)
+                             : (float)P.mu_ref;
+        float mart = 0.f;
+        if (P.art_visc) {
+            const float aS = sqrtf((float)P.gamma * me.w / me.x);
+            const float a = 0.05f * aS / HX * 0.70710678f;
+            if (-divU > a) {
+                const float tmp = divU * divU - a * a;
+                if (tmp > 0.f) mart = 0.5f * me.x * (HX * HX * 0.5f) * sqrtf(tmp) * 1.0e-5f;
+            }
+        }
+        const float mue = mu + mart;
+        diff[1] = mue * lap[0];
+        diff[2] = mue * lap[1];
+        diff[3] = mue * lap[2];
+    }
+}
+
+// One edge's share of the Green-Gauss sums of the diffusion source, seen
+// from the cell whose inward normal (nx, ny) it has: the first-gradient node
+// means A, B of the edge's two nodes give the Laplacian terms
+// 0.5 (A + B).(-ny, -nx) side of each variable (calcDiffTerm.jl:88-104,
+// gradX paired with -ny), and the node velocities a, b the velocity
+// divergence term 0.5 (a + b).(-nx, -ny) side of the artificial viscosity.
+// The other cell of the edge sees the exact negation.
+__device__ __forceinline__ float4 visc_face_f(const NodeGradF &A, const NodeGradF &B, const float4 &a,
+                                              const float4 &b, float nx, float ny, float side, bool art) {
+    const float cx = -ny * 0.5f * side, cy = -nx * 0.5f * side;
+    float4 r;
+    r.x = (A.ru.x + B.ru.x) * cx + (A.ru.y + B.ru.y) * cy;
+    r.y = (A.rv.x + B.rv.x) * cx + (A.rv.y + B.rv.y) * cy;
+    r.z = (A.re.x + B.re.x) * cx + (A.re.y + B.re.y) * cy;
+    r.w = art ? (a.y + b.y) * cy + (a.z + b.z) * cx : 0.f;
+    return r;
+}
+
 // Diffusion source (calcDiffTerm.jl:88-113 and the extension models) in FP32.
 template <bool QUAD>
 __device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &s, const DevCase &P, int64_t g,
@@ -129,36 +181,8 @@ __device__ __forceinline__ void diff_source_f(const DevMesh &m, const DevState &
         }
     }
     const float rA = ld_once(m.rareaf + g);
-    float lap[3];
-#pragma unroll
-    for (int v = 0; v < 3; ++v) lap[v] = (sx[v] + sy[v]) * rA;
-    const float T = me.w / me.x / (float)P.R;
-    diff[0] = 0.f;
-    if (P.visc_model == VISC_REFERENCE) {
-        const float mu = (float)P.mu_ref;
-        diff[1] = mu * lap[0];
-        diff[2] = mu * lap[1];
-        diff[3] = mu * (float)air_conductivity((double)T) * lap[2];
-    } else {
-        const float mu = (P.visc_model == VISC_SUTHERLAND)
-                             ? (float)P.mu_ref * (sutherland(T) / (float)P.suth_ref)
-                             : (float)P.mu_ref;
-        float mart = 0.f;
-        if (art) {
-            const float HX = ld_once(m.hxf + g);
-            const float divU = (du + dv) * rA;
-            const float aS = sqrtf((float)P.gamma * me.w / me.x);
-            const float a = 0.05f * aS / HX * 0.70710678f;
-            if (-divU > a) {
-                const float tmp = divU * divU - a * a;
-                if (tmp > 0.f) mart = 0.5f * me.x * (HX * HX * 0.5f) * sqrtf(tmp) * 1.0e-5f;
-            }
-        }
-        const float mue = mu + mart;
-        diff[1] = mue * lap[0];
-        diff[2] = mue * lap[1];
-        diff[3] = mue * lap[2];
-    }
+    const float lap[3] = {(sx[0] + sy[0]) * rA, (sx[1] + sy[1]) * rA, (sx[2] + sy[2]) * rA};
+    visc_source_f(P, me, lap, (du + dv) * rA, art ? ld_once(m.hxf + g) : 0.f, diff);
 }
 
 // FP32 increment, FP64 accumulation of the Euler update
