@@ -713,6 +713,12 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
             tf_off[t + 1] = (int64_t)tf_rec.size();
         }
         h->nfaces = (int64_t)tf_rec.size();
+        if (h->nfaces >= (int64_t)INT32_MAX) {  // the tile kernels index faces with 32 bits
+            if (h->own_stream) cudaStreamDestroy(h->stream);
+            delete h;
+            return fail(nullptr, GD2D_ERR_ARG, "%lld tile faces: more than the tile-face loop supports",
+                        (long long)tf_rec.size());
+        }
     }
 
     // ------------------------------------------------------- device
@@ -810,7 +816,6 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         int64_t *d_tfo;
         int4 *d_tfr;
         int2 *d_tfq = nullptr;
-        double *d_tnx, *d_tny, *d_tlen;
         ALLOC(d_tfo, tf_off.size()); UPLOAD(d_tfo, tf_off);
         ALLOC(d_tfr, tf_rec.size()); UPLOAD(d_tfr, tf_rec);
         if (h->quads) { ALLOC(d_tfq, tf_q.size()); UPLOAD(d_tfq, tf_q); }
@@ -819,12 +824,9 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
             ALLOC(d_tfe, tf_e.size()); UPLOAD(d_tfe, tf_e);
             m.tf_e = d_tfe;
         }
-        if (!h->mixed) {
-            ALLOC(d_tnx, tf_nx.size()); UPLOAD(d_tnx, tf_nx);
-            ALLOC(d_tny, tf_ny.size()); UPLOAD(d_tny, tf_ny);
-            ALLOC(d_tlen, tf_len.size()); UPLOAD(d_tlen, tf_len);
-            m.tf_nx = d_tnx; m.tf_ny = d_tny; m.tf_len = d_tlen;
-        } else {
+        if (h->mixed) {
+            // (the FP64 tile kernel reads the face geometry from the per-cell
+            // planes, which its viscous source reads too)
             auto to_f = [](const std::vector<double> &v) {
                 std::vector<float> f(v.size());
                 for (size_t i = 0; i < v.size(); ++i) f[i] = (float)v[i];

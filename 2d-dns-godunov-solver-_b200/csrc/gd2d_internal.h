@@ -104,12 +104,12 @@ struct DevMesh {
     // [tf_off[t], tf_off[t+1]); tf_rec = (neighbour code, packed slots, dn, up)
     // with packed = la | ka << 10 | (lb + 1) << 12 | kb << 22 | quad << 24
     // (lb + 1 = 0: the face is not shared with another cell of the tile);
-    // tf_q = (dn2, up2) for quads; the face geometry of slot (la, ka)
+    // tf_q = (dn2, up2) for quads; mixed precision: the face geometry of
+    // slot (la, ka) (the FP64 kernel reads it from the per-cell planes)
     const int64_t *tf_off;               // [ntiles + 1]
     const int4 *tf_rec;
     const int2 *tf_q;
     const int2 *tf_e;                    // (viscous) edge node pair of slot (la, ka)
-    const double *tf_nx, *tf_ny, *tf_len;
     const float *tf_nxf, *tf_nyf, *tf_lenf;
 };
 

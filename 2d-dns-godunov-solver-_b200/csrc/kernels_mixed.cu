@@ -63,11 +63,12 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
                 W0 = avg4(W0, nodeP[up2.x]); W1 = avg4(W1, nodeP[up2.y]); W2 = avg4(W2, nodeP[up2.z]);
             }
             float F[4], f[4];
-            face_flux_pre<FLUX>(m, P, g, 0, nb.x, R0, D0, W0, nx0, ny0, l0, uL, hx_own, h0, t, g2, F);
-            face_flux_pre<FLUX>(m, P, g, 1, nb.y, R1, D1, W1, nx1, ny1, l1, uL, hx_own, h1, t, g2, f);
+            const FaceConstsF kc = face_consts_f(P);
+            face_flux_pre<FLUX>(m, P, kc, g, 0, nb.x, R0, D0, W0, nx0, ny0, l0, uL, hx_own, h0, t, F);
+            face_flux_pre<FLUX>(m, P, kc, g, 1, nb.y, R1, D1, W1, nx1, ny1, l1, uL, hx_own, h1, t, f);
 #pragma unroll
             for (int v = 0; v < 4; ++v) F[v] += f[v];
-            face_flux_pre<FLUX>(m, P, g, 2, nb.z, R2, D2, W2, nx2, ny2, l2, uL, hx_own, h2, t, g2, f);
+            face_flux_pre<FLUX>(m, P, kc, g, 2, nb.z, R2, D2, W2, nx2, ny2, l2, uL, hx_own, h2, t, f);
 #pragma unroll
             for (int v = 0; v < 4; ++v) F[v] += f[v];
             if (QUAD && is_quad) {

@@ -55,15 +55,16 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
         const int c = m.tile_case[tile];
         const DevCase &P = m.cases[c];
         const double t = s.cstate[c].t;
-        const bool venkat = P.limiter == LIM_VENKAT;
+        const FaceConstsF kc = face_consts_f(P);
+        const bool venkat = kc.lim == LIM_VENKAT;
         const bool art = VISC && P.visc_model != VISC_REFERENCE && P.art_visc;
+        // face indices fit 32 bits (setup checks the total)
+        const int fb = (int)f0 + (int)threadIdx.x, fe = (int)f1;
         __syncthreads();
-        const float gam = (float)P.gamma;
-        const float g2 = 2.f * (gam - 1.f) / (gam + 1.f);
         if (VISC) {
             // the face records and geometry are loaded cached here: the flux
             // pass reads them again
-            for (int64_t f = f0 + threadIdx.x; f < f1; f += B) {
+            for (int f = fb; f < fe; f += B) {
                 const TileFace tf = unpack_tile_face(m.tf_rec[f].y);
                 const float nxf = m.tf_nxf[f], nyf = m.tf_nyf[f], lenf = m.tf_lenf[f];
                 const int2 e = ld_once(m.tf_e + f);
@@ -75,7 +76,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
                 if (tf.lbp) s_visc[tf.kb][tf.lbp - 1] = make_float4(-vv.x, -vv.y, -vv.z, -vv.w);
             }
         }
-        for (int64_t f = f0 + threadIdx.x; f < f1; f += B) {
+        for (int f = fb; f < fe; f += B) {
             const int4 rec = ld_once(m.tf_rec + f);
             const TileFace tf = unpack_tile_face(rec.y);
             const float4 a4 = s_prim[tf.la];
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
             float4 r = a4, dd = a4, uu = a4;
             float hxR = hx_own;
             if (rec.x >= 0) {
-                const int64_t lr = (int64_t)rec.x - base;
+                const int lr = rec.x - (int)base;
                 if (lr >= 0 && lr < B) {
                     r = s_prim[lr];
                     if (venkat) hxR = s_hx[lr];
@@ -102,7 +103,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
                 }
             }
             float fv[4];
-            face_flux_pre<FLUX>(m, P, base + tf.la, tf.ka, rec.x, r, dd, uu, nxf, nyf, lenf, uL, hx_own, hxR, t, g2,
+            face_flux_pre<FLUX>(m, P, kc, base + tf.la, tf.ka, rec.x, r, dd, uu, nxf, nyf, lenf, uL, hx_own, hxR, t,
                                 fv);
             s_flux[tf.ka][tf.la] = make_float4(fv[0], fv[1], fv[2], fv[3]);
             if (tf.lbp) s_flux[tf.kb][tf.lbp - 1] = make_float4(-fv[0], -fv[1], -fv[2], -fv[3]);

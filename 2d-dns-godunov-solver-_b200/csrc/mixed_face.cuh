@@ -61,14 +61,99 @@ __device__ __forceinline__ void face_flux_f(const DevMesh &m, const DevCase &P, 
     face_flux_fn<FLUX, float>(UpR, UpL, nx, ny, side, (float)P.gamma, g2, f);
 }
 
-// The same face with every gathered input already in registers: r = the
+// Per-case constants of the FP32 face arithmetic, read from the case record
+// once per tile rather than once per face.
+struct FaceConstsF {
+    float gam;  // gamma
+    float g2;   // 2 (gamma - 1) / (gamma + 1)
+    float hk;   // gamma / (gamma - 1): p/rho + p/rho/(gamma-1) = (p/rho) hk
+    float vK;   // Venkatakrishnan K
+    float ksi;  // Minmod constant
+    int lim;    // limiter kind
+};
+__device__ __forceinline__ FaceConstsF face_consts_f(const DevCase &P) {
+    FaceConstsF k;
+    k.gam = (float)P.gamma;
+    k.g2 = (float)(2.0 * (P.gamma - 1.0) / (P.gamma + 1.0));
+    k.hk = (float)(P.gamma / (P.gamma - 1.0));
+    k.vK = (float)P.venkat_K;
+    k.ksi = (float)P.ksi;
+    k.lim = P.limiter;
+    return k;
+}
+
+// The limiters of the mixed path without the reference's exact-rounding
+// constraints: branch-free selects and fast division.
+// Venkatakrishnan in the two-argument slot (same function as lim_venkat).
+__device__ __forceinline__ float venkat_fast(float o, float c, float e2) {
+    c = (o * c < 0.f) ? 0.f : c;
+    const float oo = o * o;
+    const float den = c * c + 2.f * oo + o * c + e2;  // >= 0
+    const float num = (c * c + e2) * o + 2.f * oo * c;
+    return den > 0.f ? __fdividef(num, den) : 0.f;
+}
+// Minmod_Limiter (limiters.jl:33-35).
+__device__ __forceinline__ float minmod_fast(float x, float y, float c) {
+    const float sx = x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f), sy = y > 0.f ? 1.f : (y < 0.f ? -1.f : 0.f);
+    return __fdividef((sx + sy) * fabsf(x * y), fabsf(x) + fabsf(y) + c);
+}
+
+// AUSM+ (Liou 1996; the reference's variant with a12 = the smaller of the
+// two numerical sound speeds, AUSMflux2dFast.jl:87-175) in FP32 for the
+// mixed path: the same formulas, regrouped where that saves work --
+// p/rho + p/rho/(gamma-1) = (p/rho) gamma/(gamma-1), a~ = s min(1, s/|u.n|)
+// = min(s, s^2/|u.n|), the split Mach and pressure polynomials as selects,
+// (m + |m|)/2 = max(m, 0) -- with fast division and square root.
+// L is the neighbour's reconstruction and R the cell's own, as
+// computeslope2d.jl:129 passes them.
+__device__ __forceinline__ float mach_p(float M) {  // M+ with beta = 1/8
+    const float q = M * M - 1.f;
+    return fabsf(M) >= 1.f ? fmaxf(M, 0.f) : 0.25f * (M + 1.f) * (M + 1.f) + 0.125f * q * q;
+}
+__device__ __forceinline__ float mach_m(float M) {  // M- with beta = 1/8
+    const float q = M * M - 1.f;
+    return fabsf(M) >= 1.f ? fminf(M, 0.f) : -0.25f * (M - 1.f) * (M - 1.f) - 0.125f * q * q;
+}
+__device__ __forceinline__ float pres_p(float M) {  // P+ with alpha = 3/16
+    const float q = M * M - 1.f;
+    return fabsf(M) >= 1.f ? (M > 0.f ? 1.f : 0.f)
+                           : 0.25f * (M + 1.f) * (M + 1.f) * (2.f - M) + 0.1875f * M * q * q;
+}
+__device__ __forceinline__ float pres_m(float M) {  // P- with alpha = 3/16
+    const float q = M * M - 1.f;
+    return fabsf(M) >= 1.f ? (M < 0.f ? 1.f : 0.f)
+                           : 0.25f * (M - 1.f) * (M - 1.f) * (2.f + M) - 0.1875f * M * q * q;
+}
+__device__ __forceinline__ void ausm_plus_fast(const float *L, const float *R, float nx, float ny, float side,
+                                               const FaceConstsF &k, float *flux) {
+    const float rL = L[0], uL = L[1], vL = L[2], pL = L[3];
+    const float rR = R[0], uR = R[1], vR = R[2], pR = R[3];
+    const float htL = fmaf(0.5f, uL * uL + vL * vL, __fdividef(pL, rL) * k.hk);
+    const float htR = fmaf(0.5f, uR * uR + vR * vR, __fdividef(pR, rR) * k.hk);
+    const float s2L = k.g2 * htL, s2R = k.g2 * htR;
+    const float vnL = uL * nx + vL * ny, vnR = uR * nx + vR * ny;
+    const float aL = fminf(sqrtf(s2L), __fdividef(s2L, fabsf(vnL)));
+    const float aR = fminf(sqrtf(s2R), __fdividef(s2R, fabsf(vnR)));
+    const float a12 = fminf(aL, aR);
+    const float ia = __fdividef(1.f, a12);
+    const float ML = vnL * ia, MR = vnR * ia;
+    const float mdot = mach_p(ML) + mach_m(MR);
+    const float p12 = pres_p(ML) * pL + pres_m(MR) * pR;
+    const float mp = a12 * fmaxf(mdot, 0.f) * rL, mm = a12 * fminf(mdot, 0.f) * rR;
+    flux[0] = -(mp + mm) * side;
+    flux[1] = -(mp * uL + mm * uR + p12 * nx) * side;
+    flux[2] = -(mp * vL + mm * vR + p12 * ny) * side;
+    flux[3] = -(mp * htL + mm * htR) * side;
+}
+
+// The face with every gathered input already in registers: r = the
 // neighbour's primitives, d/u = down/up node primitives (quads: averaged),
 // geometry (nx, ny, side).  Boundary faces ignore r, d, u.
 template <int FLUX>
-__device__ __forceinline__ void face_flux_pre(const DevMesh &m, const DevCase &P, int64_t g, int k, int nbk,
-                                              const float4 &r, const float4 &dd, const float4 &uu, float nx, float ny,
-                                              float side, const float *uL, float hx_own, float hxR, double t, float g2,
-                                              float *f) {
+__device__ __forceinline__ void face_flux_pre(const DevMesh &m, const DevCase &P, const FaceConstsF &kc, int64_t g,
+                                              int k, int nbk, const float4 &r, const float4 &dd, const float4 &uu,
+                                              float nx, float ny, float side, const float *uL, float hx_own,
+                                              float hxR, double t, float *f) {
     float uR[4], uUp[4], uDn[4];
     if (nbk >= 0) {
         uR[0] = r.x; uR[1] = r.y; uR[2] = r.z; uR[3] = r.w;
@@ -80,26 +165,30 @@ __device__ __forceinline__ void face_flux_pre(const DevMesh &m, const DevCase &P
         for (int v = 0; v < 4; ++v) { uDn[v] = uL[v]; uUp[v] = uR[v]; }
     }
     float UpL[4], UpR[4];
-    if (P.limiter == LIM_VENKAT) {
-        const float K = (float)P.venkat_K;
-        const float KL = K * hx_own, KR = K * hxR;
+    if (kc.lim == LIM_VENKAT) {
+        const float KL = kc.vK * hx_own, KR = kc.vK * hxR;
         const float e2L = KL * KL * KL, e2R = KR * KR * KR;
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
             const float sc = 0.5f * (uL[v] * uL[v] + uR[v] * uR[v]);
-            UpL[v] = uL[v] + 0.5f * lim_venkat(uL[v] - uDn[v], uR[v] - uL[v], e2L * sc);
-            UpR[v] = uR[v] + 0.5f * lim_venkat(uR[v] - uUp[v], uL[v] - uR[v], e2R * sc);
+            UpL[v] = uL[v] + 0.5f * venkat_fast(uL[v] - uDn[v], uR[v] - uL[v], e2L * sc);
+            UpR[v] = uR[v] + 0.5f * venkat_fast(uR[v] - uUp[v], uL[v] - uR[v], e2R * sc);
         }
-    } else {
-        const int lk = P.limiter;
-        const float ksi = (float)P.ksi;
+    } else if (kc.lim == LIM_MINMOD) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            UpL[v] = uL[v] + 0.5f * limiter(lk, uL[v] - uDn[v], uR[v] - uL[v], ksi);
-            UpR[v] = uR[v] - 0.5f * limiter(lk, uR[v] - uL[v], uUp[v] - uR[v], ksi);
+            UpL[v] = uL[v] + 0.5f * minmod_fast(uL[v] - uDn[v], uR[v] - uL[v], kc.ksi);
+            UpR[v] = uR[v] - 0.5f * minmod_fast(uR[v] - uL[v], uUp[v] - uR[v], kc.ksi);
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            UpL[v] = uL[v] + 0.5f * limiter(kc.lim, uL[v] - uDn[v], uR[v] - uL[v], kc.ksi);
+            UpR[v] = uR[v] - 0.5f * limiter(kc.lim, uR[v] - uL[v], uUp[v] - uR[v], kc.ksi);
         }
     }
-    face_flux_fn<FLUX, float>(UpR, UpL, nx, ny, side, (float)P.gamma, g2, f);
+    if (FLUX == FLUX_AUSM) ausm_plus_fast(UpR, UpL, nx, ny, side, kc, f);
+    else face_flux_fn<FLUX, float>(UpR, UpL, nx, ny, side, kc.gam, kc.g2, f);
 }
 
 __device__ __forceinline__ float4 avg4(const float4 &a, const float4 &b) {

@@ -321,7 +321,7 @@ __device__ __forceinline__ void diff_source(const DevMesh &m, const DevState &s,
     const bool art = (P.visc_model != VISC_REFERENCE) && P.art_visc;
     for (int k = 0; k < nf; ++k) {
         const int64_t o = (int64_t)k * m.Nc + g;
-        const double side = ld_once(m.len + o), nx = ld_once(m.nx + o), ny = ld_once(m.ny + o);
+        const double side = m.len[o], nx = m.nx[o], ny = m.ny[o];
         const int2 e = ld_once(m.c2n + o);
         const NodeGrad A = s.nodeG[e.x], B = s.nodeG[e.y];
         double fx, fy;
@@ -541,8 +541,11 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
             int2 q2 = make_int2(0, 0);
             if (QUAD && tf.quad) q2 = m.tf_q[f];
             double fv[4];
+            // the face geometry of slot (la, ka) from the per-cell planes,
+            // cached: the viscous source reads the same lines again
+            const int64_t og = (int64_t)tf.ka * m.Nc + base + tf.la;
             face_flux_at<FLUX, QUAD>(m, P, s.nodeP, base + tf.la, tf.ka, rec.x, rec.z, rec.w, q2.x, q2.y,
-                                     QUAD && tf.quad, uL, r, hx_own, hxR, ld_once(m.tf_len + f), ld_once(m.tf_nx + f), ld_once(m.tf_ny + f), t,
+                                     QUAD && tf.quad, uL, r, hx_own, hxR, m.len[og], m.nx[og], m.ny[og], t,
                                      g2, fv);
             s_flux[tf.ka][tf.la] = make_double4(fv[0], fv[1], fv[2], fv[3]);
             if (tf.lbp) s_flux[tf.kb][tf.lbp - 1] = make_double4(-fv[0], -fv[1], -fv[2], -fv[3]);
@@ -553,17 +556,26 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
         // held in registers through the face phase)
         const double4 me = s_prim[threadIdx.x];
         const double dt = s.cstate[c].dt;
-        const int4 nb = ld_once(m.nbr + g);
-        const bool is_quad = QUAD && (nb.w != kAbsent);
+        // triangles: the viscous source is evaluated for padding cells too
+        // (node 0 in their edge slots, zero area; the result is unused), and
+        // a padding cell is told by its zero inverse area; quads read the
+        // neighbour record, which also tells triangles from quads
+        bool live = true, is_quad = false;
+        if (QUAD) {
+            const int4 nb = ld_once(m.nbr + g);
+            live = nb.x != kAbsent;
+            is_quad = nb.w != kAbsent;
+        }
         double diff[4] = {0.0, 0.0, 0.0, 0.0};
-        if (VISC && nb.x != kAbsent) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
+        if (VISC && live) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
         // the update's own loads go out before the barrier (padded arrays:
         // in bounds for padding cells, whose values are not used)
         const CellIn cin = load_cell_in(m, s, g);
+        if (!QUAD) live = cin.rarea != 0.0;
         __syncthreads();
         Part part;
         part.init();
-        if (nb.x != kAbsent) {
+        if (live) {
             const double4 a0 = s_flux[0][threadIdx.x], a1 = s_flux[1][threadIdx.x], a2 = s_flux[2][threadIdx.x];
             double F[4] = {a0.x + a1.x, a0.y + a1.y, a0.z + a1.z, a0.w + a1.w};
             F[0] = F[0] + a2.x; F[1] = F[1] + a2.y; F[2] = F[2] + a2.z; F[3] = F[3] + a2.w;
