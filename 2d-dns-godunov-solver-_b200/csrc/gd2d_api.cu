@@ -9,9 +9,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <thread>
@@ -54,6 +57,71 @@ struct DevBuffers {
         for (void *p : all) cudaFree(p);
         all.clear();
     }
+};
+
+// Host worker threads of a handle's staged transfers, started on first use
+// and kept until the handle is destroyed, so that a transfer does not pay
+// the start-up of its threads (tens of microseconds each).  run() hands out
+// items 0..n-1 in increasing order to the workers and the calling thread and
+// returns once every item is done.
+class StagePool {
+  public:
+    ~StagePool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            quit_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    void run(int device, unsigned workers, unsigned n, const std::function<void(unsigned)> &fn) {
+        if (th_.size() < workers) start(device, workers);
+        std::unique_lock<std::mutex> lk(mu_);
+        job_ = &fn;
+        njobs_ = n;
+        next_ = 0;
+        finished_ = 0;
+        ++gen_;
+        cv_.notify_all();
+        drain(lk);
+        done_cv_.wait(lk, [&] { return finished_ == njobs_; });
+        job_ = nullptr;
+    }
+
+  private:
+    void start(int device, unsigned workers) {
+        while (th_.size() < workers) {
+            th_.emplace_back([this, device] {
+                cudaSetDevice(device);  // the DMAs are queued from these threads
+                uint64_t seen = 0;
+                std::unique_lock<std::mutex> lk(mu_);
+                for (;;) {
+                    cv_.wait(lk, [&] { return quit_ || (gen_ != seen && job_ != nullptr); });
+                    if (quit_) return;
+                    seen = gen_;
+                    drain(lk);
+                }
+            });
+        }
+    }
+    // Takes items until none is left (mu_ held on entry and exit).
+    void drain(std::unique_lock<std::mutex> &lk) {
+        while (job_ && next_ < njobs_) {
+            const unsigned k = next_++;
+            const std::function<void(unsigned)> *fn = job_;
+            lk.unlock();
+            (*fn)(k);
+            lk.lock();
+            if (++finished_ == njobs_) done_cv_.notify_all();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(unsigned)> *job_ = nullptr;
+    unsigned njobs_ = 0, next_ = 0, finished_ = 0;
+    uint64_t gen_ = 0;
+    bool quit_ = false;
 };
 
 }  // namespace
@@ -101,6 +169,8 @@ struct gd2d_handle {
     bool split_stage_done = false, split_diff_valid = false;
     std::vector<CaseState> cs_host;  // host copy: steps taken per case (advanced by propagate)
     DevStats *ring_host = nullptr;    // page-locked, mapped copy of the statistics ring
+    std::vector<cudaEvent_t> slice_ev;  // one per slice of a staged download
+    StagePool pool;                     // host threads of the staged transfers
     std::string err;
 };
 
@@ -908,16 +978,18 @@ static int copy_sync(gd2d_handle *h, void *dst, const void *src, size_t bytes, c
 }
 
 // Transfers between a caller's host columns and the device stage go
-// through the page-locked host stage in slices of >= 4 MB, one worker
-// thread per slice (at most 8): a worker's host copy and its slice's DMA
-// overlap the other workers' copies, and the copies together use more of
-// the host memory bandwidth than one thread can.  The stage holds a case's
+// through the page-locked host stage in slices of 2 MB, handed out in order
+// to the handle's worker threads (StagePool, at most 8 threads with the
+// caller): uploads copy a slice into the stage and queue its DMA at once,
+// so the DMA engine starts after the first slice and streams while the
+// other slices are copied; downloads queue every slice's DMA first and copy
+// each slice out as soon as its event completes.  The stage holds a case's
 // 4 columns back to back, element v * n + i for row i of column v.
-static unsigned stage_workers(size_t bytes) {
-    const size_t kPart = (size_t)4 << 20;
-    unsigned nt = std::thread::hardware_concurrency();
-    nt = std::max(1u, std::min(nt, 8u));
-    return (unsigned)std::min<size_t>(nt, std::max<size_t>(1, bytes / kPart));
+constexpr size_t kSliceElems = (size_t)1 << 18;  // 2 MB of doubles
+
+static unsigned stage_threads() {
+    const unsigned nt = std::thread::hardware_concurrency();
+    return std::max(1u, std::min(nt, 8u));
 }
 
 // Elements [b0, b1) of the stage, copied from (to_stage) or to the columns.
@@ -936,23 +1008,14 @@ static int staged_upload(gd2d_handle *h, const double *const src[4], int64_t n) 
     double *cols[4] = {const_cast<double *>(src[0]), const_cast<double *>(src[1]), const_cast<double *>(src[2]),
                        const_cast<double *>(src[3])};
     const size_t total = 4 * (size_t)n;
-    const unsigned nt = stage_workers(sizeof(double) * total);
-    std::vector<cudaError_t> err(nt, cudaSuccess);
-    auto work = [&](unsigned k) {
-        const size_t b0 = total * k / nt, b1 = total * (k + 1) / nt;
+    const unsigned ns = (unsigned)((total + kSliceElems - 1) / kSliceElems);
+    std::vector<cudaError_t> err(ns, cudaSuccess);
+    h->pool.run(h->device, stage_threads() - 1, ns, [&](unsigned k) {
+        const size_t b0 = (size_t)k * kSliceElems, b1 = std::min(total, b0 + kSliceElems);
         stage_copy(h->h_stage, cols, n, b0, b1, true);
-        if (nt > 1) err[k] = cudaSetDevice(h->device);
-        if (err[k] == cudaSuccess)
-            err[k] = cudaMemcpyAsync(h->d_stage + b0, h->h_stage + b0, sizeof(double) * (b1 - b0),
-                                     cudaMemcpyHostToDevice, h->stream);
-    };
-    if (nt == 1) {
-        work(0);
-    } else {
-        std::vector<std::thread> th;
-        for (unsigned k = 0; k < nt; ++k) th.emplace_back(work, k);
-        for (auto &t : th) t.join();
-    }
+        err[k] = cudaMemcpyAsync(h->d_stage + b0, h->h_stage + b0, sizeof(double) * (b1 - b0),
+                                 cudaMemcpyHostToDevice, h->stream);
+    });
     for (cudaError_t e : err)
         if (e != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "staged upload: %s", cudaGetErrorString(e));
     return GD2D_OK;
@@ -963,37 +1026,29 @@ static int staged_upload(gd2d_handle *h, const double *const src[4], int64_t n) 
 static int staged_download(gd2d_handle *h, double *dst, int64_t n) {
     double *cols[4] = {dst, dst + n, dst + 2 * n, dst + 3 * n};
     const size_t total = 4 * (size_t)n;
-    const unsigned nt = stage_workers(sizeof(double) * total);
-    std::vector<cudaEvent_t> ev(nt, nullptr);
+    const unsigned ns = (unsigned)((total + kSliceElems - 1) / kSliceElems);
     cudaError_t e = cudaSuccess;
-    for (unsigned k = 0; k < nt && e == cudaSuccess; ++k) {
-        const size_t b0 = total * k / nt, b1 = total * (k + 1) / nt;
-        e = cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(h->h_stage + b0, h->d_stage + b0, sizeof(double) * (b1 - b0), cudaMemcpyDeviceToHost,
-                                h->stream);
-        if (e == cudaSuccess) e = cudaEventRecord(ev[k], h->stream);
+    while (e == cudaSuccess && h->slice_ev.size() < ns) {
+        cudaEvent_t x = nullptr;
+        e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+        if (e == cudaSuccess) h->slice_ev.push_back(x);
     }
-    std::vector<cudaError_t> err(nt, e);
-    if (e == cudaSuccess) {
-        auto work = [&](unsigned k) {
-            const size_t b0 = total * k / nt, b1 = total * (k + 1) / nt;
-            if (nt > 1) err[k] = cudaSetDevice(h->device);
-            if (err[k] == cudaSuccess) err[k] = cudaEventSynchronize(ev[k]);
-            if (err[k] == cudaSuccess) stage_copy(h->h_stage, cols, n, b0, b1, false);
-        };
-        if (nt == 1) {
-            work(0);
-        } else {
-            std::vector<std::thread> th;
-            for (unsigned k = 0; k < nt; ++k) th.emplace_back(work, k);
-            for (auto &t : th) t.join();
-        }
-    } else {
+    for (unsigned k = 0; k < ns && e == cudaSuccess; ++k) {
+        const size_t b0 = (size_t)k * kSliceElems, b1 = std::min(total, b0 + kSliceElems);
+        e = cudaMemcpyAsync(h->h_stage + b0, h->d_stage + b0, sizeof(double) * (b1 - b0), cudaMemcpyDeviceToHost,
+                            h->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(h->slice_ev[k], h->stream);
+    }
+    if (e != cudaSuccess) {
         cudaStreamSynchronize(h->stream);  // nothing queued above may outlive the call
+        return fail(h, GD2D_ERR_CUDA, "staged download: %s", cudaGetErrorString(e));
     }
-    for (cudaEvent_t x : ev)
-        if (x) cudaEventDestroy(x);
+    std::vector<cudaError_t> err(ns, cudaSuccess);
+    h->pool.run(h->device, stage_threads() - 1, ns, [&](unsigned k) {
+        const size_t b0 = (size_t)k * kSliceElems, b1 = std::min(total, b0 + kSliceElems);
+        err[k] = cudaEventSynchronize(h->slice_ev[k]);
+        if (err[k] == cudaSuccess) stage_copy(h->h_stage, cols, n, b0, b1, false);
+    });
     for (cudaError_t x : err)
         if (x != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "staged download: %s", cudaGetErrorString(x));
     return GD2D_OK;
@@ -1584,6 +1639,7 @@ int gd2d_destroy(gd2d_handle *h) {
     drop_graph(h);
     for (auto &e : h->ev_total) if (e) cudaEventDestroy(e);
     for (auto &e : h->ev_eager) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : h->slice_ev) cudaEventDestroy(e);
     if (h->ring_host) cudaFreeHost(h->ring_host);
     if (h->h_stage) cudaFreeHost(h->h_stage);
     h->buf.free_all();

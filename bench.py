@@ -39,8 +39,12 @@ import __graft_entry__ as graft  # noqa: E402
 
 # Algorithmic bytes per cell-step (compulsory traffic of the reference
 # dataflow: state read+write, face geometry, connectivity, node-average
-# cluster data; intermediates counted zero).
+# cluster data; intermediates counted zero) for the whole step ...
 ALG_BYTES = {("f64", False): 216, ("f64", True): 248, ("mixed", False): 164, ("mixed", True): 192}
+# ... and for the fused cell kernel alone: the same without the node pass's
+# cluster ids and weights, 0.5 nodes per cell x 6 cells x (4 + weight bytes)
+# = 36 B in FP64 and 24 B in the mixed path.
+CELL_ALG_BYTES = {("f64", False): 180, ("f64", True): 212, ("mixed", False): 140, ("mixed", True): 168}
 
 # DRAM bytes per cell of one cell-kernel launch on the viscous cylinder,
 # measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one
@@ -279,7 +283,8 @@ def mixed_variant(pkg, items, s64, args, peak):
     sm.propagate2d(args.steps)
     tot, cell_ms, _ = sm.last_timing()
     value = mesh.nCells * args.steps / (tot / 1e3) / 1e6
-    alg = ALG_BYTES[("mixed", cfg.get("viscosity", "none") != "none")]
+    visc = cfg.get("viscosity", "none") != "none"
+    alg, calg = ALG_BYTES[("mixed", visc)], CELL_ALG_BYTES[("mixed", visc)]
     # error run: both paths from the initial state
     n_err = args.error_steps
     sm.createFields2d(0, *prims)
@@ -304,14 +309,27 @@ def mixed_variant(pkg, items, s64, args, peak):
     tscale = [abs(t064[0]), math.hypot(t064[1], t064[2]), math.hypot(t064[1], t064[2]), abs(t064[3])]
     drift = [abs((hm["totals"][v] - t0m[v]) - (h64["totals"][v] - t064[v])) / max(tscale[v], 1e-300)
              for v in range(4)]
+    # the densityConstrained clamp (evaluate2d.jl:63-77): cells sitting at
+    # the lower bound after the error run, and their share of the mass
+    clamp = None
+    if cfg.get("densityConstrained", 0):
+        lo = cfg.get("minDensityConstrained", 0.01)
+        A = mesh.cell_areas
+        clamp = {"bound": lo}
+        for tag, U in (("fp64", U64), ("mixed", Um)):
+            at = U[:, 0] <= lo
+            clamp[tag] = {"cells_at_bound": int(at.sum()), "cell_fraction": float(at.mean()),
+                          "mass_fraction": float((U[at, 0] * A[at]).sum() / (U[:, 0] * A).sum())}
     sm.close()
     return {"value": value, "unit": "Mcell-steps/s", "ms_per_step": tot / args.steps, "cell_kernel_ms": cell_ms,
-            "roofline": {"achieved": alg * mesh.nCells / (cell_ms / 1e3) / 1e9 if cell_ms else None, "peak": peak,
-                         "frac": (alg * mesh.nCells / (cell_ms / 1e3) / 1e9 / peak) if cell_ms else None,
-                         "alg_bytes_per_cell": alg},
+            "roofline": {"achieved": calg * mesh.nCells / (cell_ms / 1e3) / 1e9 if cell_ms else None, "peak": peak,
+                         "frac": (calg * mesh.nCells / (cell_ms / 1e3) / 1e9 / peak) if cell_ms else None,
+                         "alg_bytes_per_cell": calg, "step_alg_bytes_per_cell": alg,
+                         "step_frac": alg * mesh.nCells / (tot / args.steps / 1e3) / 1e9 / peak},
             "error_vs_fp64": {"steps": n_err, "momentum_scaled_by": "momentum magnitude",
                               "l2_rel": [float(x) for x in l2], "linf_rel": [float(x) for x in linf],
-                              "vars": ["rho", "rho_u", "rho_v", "E"], "totals_drift_rel": drift}}
+                              "vars": ["rho", "rho_u", "rho_v", "E"], "totals_drift_rel": drift},
+            "density_clamp": clamp}
 
 
 def batched_mixed(pkg, items, s64, args, peak, kind):
@@ -336,7 +354,8 @@ def batched_mixed(pkg, items, s64, args, peak, kind):
     sm.propagate2d(args.steps)
     tot, cell_ms, launches = sm.last_timing()
     value = cells * args.steps / (tot / 1e3) / 1e6
-    alg = ALG_BYTES[("mixed", cfgs[0].get("viscosity", "none") != "none")]
+    visc = cfgs[0].get("viscosity", "none") != "none"
+    alg, calg = ALG_BYTES[("mixed", visc)], CELL_ALG_BYTES[("mixed", visc)]
     n_err = args.error_steps
     for i, (_, _, p) in enumerate(items):
         sm.createFields2d(i, *p)
@@ -361,11 +380,11 @@ def batched_mixed(pkg, items, s64, args, peak, kind):
         per_case.append(rec)
     sm.close()
     key = "decay_rel_err" if kind == "tgv" else "rho_l2_rel_err"
-    achieved = alg * cells / (cell_ms / 1e3) / 1e9 if cell_ms else None
+    achieved = calg * cells / (cell_ms / 1e3) / 1e9 if cell_ms else None
     return {"value": value, "unit": "Mcell-steps/s", "cells": cells, "ms_per_step": tot / args.steps,
             "cell_kernel_ms": cell_ms, "gpu_launches": int(launches), "autotuned_launch": tuned,
             "roofline": {"achieved": achieved, "peak": peak, "frac": achieved / peak if achieved else None,
-                         "alg_bytes_per_cell": alg,
+                         "alg_bytes_per_cell": calg, "step_alg_bytes_per_cell": alg,
                          "step_achieved_gbs": alg * cells / (tot / args.steps / 1e3) / 1e9},
             "error_vs_fp64": {"steps": n_err, "max_" + key: max(r[key] for r in per_case), "per_case": per_case}}
 
@@ -571,8 +590,8 @@ def main():
                      "timed_region_device_ms_per_step": None}
 
     peak, peak_kind = load_peaks()
-    alg = ALG_BYTES[(args.precision, viscous)]
-    achieved = alg * cells / (cell_ms / 1e3) / 1e9 if cell_ms > 0 else None
+    alg, calg = ALG_BYTES[(args.precision, viscous)], CELL_ALG_BYTES[(args.precision, viscous)]
+    achieved = calg * cells / (cell_ms / 1e3) / 1e9 if cell_ms > 0 else None
     step_achieved = alg * cells / (ms_per_step / 1e3) / 1e9
     tpc = CELL_KERNEL_TRAFFIC.get((args.precision, args.loop)) if args.config == "cylinder" else None
     traffic = tpc * cells if tpc else None
@@ -587,7 +606,8 @@ def main():
                          "kernel": ("k_cell_step_tf" if args.loop == "tile" else "k_cell_step")
                                    + (" (mixed)" if args.precision == "mixed" else "")
                                    + " (fused reconstruction+flux+viscous+update)",
-                         "alg_bytes_per_cell": alg, "cell_kernel_ms": cell_ms, "peak_kind": peak_kind,
+                         "alg_bytes_per_cell": calg, "step_alg_bytes_per_cell": alg, "cell_kernel_ms": cell_ms,
+                         "peak_kind": peak_kind,
                          "step_achieved_gbs": step_achieved, "step_frac": step_achieved / peak},
             "e2e": {"value": e2e_val, "unit": "Mcell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps, "breakdown": dict(e2e_breakdown, timed_region_device_ms_per_step=ms_per_step)},
