@@ -60,14 +60,25 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
         const bool art = VISC && P.visc_model != VISC_REFERENCE && P.art_visc;
         // face indices fit 32 bits (setup checks the total)
         const int fb = (int)f0 + (int)threadIdx.x, fe = (int)f1;
+        // the viscous pass's first face record goes out with the staging
+        // loads and each next one before the current face's gathers, so a
+        // thread with two faces does not wait for its second record (the
+        // cached loads leave the records in L1 for the flux pass)
+        int pk = 0; int2 pe = make_int2(0, 0); float pnx = 0.f, pny = 0.f, pln = 0.f;
+        if (VISC && fb < fe) {
+            pk = m.tf_rec[fb].y; pe = ld_once(m.tf_e + fb);
+            pnx = m.tf_nxf[fb]; pny = m.tf_nyf[fb]; pln = m.tf_lenf[fb];
+        }
         __syncthreads();
         if (VISC) {
-            // the face records and geometry are loaded cached here: the flux
-            // pass reads them again
             for (int f = fb; f < fe; f += B) {
-                const TileFace tf = unpack_tile_face(m.tf_rec[f].y);
-                const float nxf = m.tf_nxf[f], nyf = m.tf_nyf[f], lenf = m.tf_lenf[f];
-                const int2 e = ld_once(m.tf_e + f);
+                const TileFace tf = unpack_tile_face(pk);
+                const float nxf = pnx, nyf = pny, lenf = pln;
+                const int2 e = pe;
+                if (f + B < fe) {
+                    pk = m.tf_rec[f + B].y; pe = ld_once(m.tf_e + f + B);
+                    pnx = m.tf_nxf[f + B]; pny = m.tf_nyf[f + B]; pln = m.tf_lenf[f + B];
+                }
                 const NodeGradF GA = s.nodeGf[e.x], GB = s.nodeGf[e.y];
                 float4 na = make_float4(0.f, 0.f, 0.f, 0.f), nb = na;
                 if (art) { na = nodeP[e.x]; nb = nodeP[e.y]; }
