@@ -980,7 +980,7 @@ static int copy_sync(gd2d_handle *h, void *dst, const void *src, size_t bytes, c
 // Transfers between a caller's host columns and the device stage go
 // through the page-locked host stage in slices of 2 MB, handed out in order
 // to the handle's worker threads (StagePool, at most 8 threads with the
-// caller): uploads copy a slice into the stage and queue its DMA at once,
+// caller; 16 measured no faster): uploads copy a slice into the stage and queue its DMA at once,
 // so the DMA engine starts after the first slice and streams while the
 // other slices are copied; downloads queue every slice's DMA first and copy
 // each slice out as soon as its event completes.  The stage holds a case's
@@ -1595,7 +1595,9 @@ int gd2d_autotune(gd2d_handle *h, int32_t steps_per_trial, gd2d_launch *chosen) 
         rc = trial(c, bestG, &ms);
         if (rc == GD2D_OK && ms < best_ms) { best = c; best_ms = ms; }
     }
+    // a graph length the caller set in the launch record is kept
     for (int G : {8, 32, 128}) {
+        if (h->launch.graph_steps > 0) break;
         if (rc != GD2D_OK || G == bestG || G > h->s.ring_len) continue;
         double ms = 0.0;
         rc = trial(best, G, &ms);

@@ -214,8 +214,9 @@ int gd2d_calc_diff_term(gd2d_handle *h, int32_t icase, double *diff);
 /* Autotuner (no counterpart in the reference, whose CPU loop has no launch
  * shape): times candidate launch shapes on this handle's own data and keeps
  * the fastest -- cell-kernel register budget (min_blocks 2/3/4) x
- * persistence, node-pass block (64/128/256), steps per graph (8/32/128) --
- * by coordinate search, `steps_per_trial` steps each (<= 0: 64).  Every
+ * persistence, node-pass block (64/128/256), steps per graph (8/32/128,
+ * unless the launch record given to gd2d_setup set graph_steps, which is
+ * kept) -- by coordinate search, `steps_per_trial` steps each (<= 0: 64).  Every
  * device array a step touches is saved first and restored after the trials,
  * so propagation continues bit-identically.  Needs gd2d_set_state on every
  * case; allocates a temporary copy of the state.  `chosen` (may be NULL)

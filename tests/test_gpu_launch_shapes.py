@@ -75,6 +75,20 @@ def test_autotune_restores_state(pkg, precision, loop):
         assert h[-1]["flowTime"] == pytest.approx(href[-1]["flowTime"], rel=1e-6)
 
 
+def test_autotune_keeps_a_set_graph_length(pkg):
+    """A graph length set in the launch record (as the batched Taylor-Green
+    workload sets 100 steps) is not searched: the autotuner keeps it and
+    tunes the rest."""
+    mesh, cfg, prims = _viscous_case(pkg)
+    s = pkg.setupSolver(mesh, cfg, graph_steps=16)
+    s.createFields2d(0, *prims)
+    chosen = s.autotune(steps_per_trial=16)
+    assert chosen["graph_steps"] == 16
+    s.propagate2d(40)
+    assert s.history(0)[-1]["step"] == 40
+    s.close()
+
+
 def test_autotune_needs_state(pkg):
     mesh, cfg, prims = _viscous_case(pkg)
     s = pkg.setupSolver(mesh, cfg)
