@@ -284,6 +284,39 @@ def propagate_until_converged(solver: "Solver", icase: int, max_steps: int, conv
     return 0
 
 
+def autotune_layout(meshes: Sequence[Mesh2d], cfgs: Sequence[Dict], prims: Sequence[Sequence[np.ndarray]],
+                    orders: Sequence[str] = ("hilbert", "rcm", "natural"), blocks: Sequence[int] = (256, 128),
+                    steps: int = 64, **launch_kw) -> Tuple[Dict, List[Dict]]:
+    """Pick the mesh ordering and the tile size (cells per block of the cell
+    kernel) by timing them.  Both are fixed when a handle is set up (they
+    decide the device layout and the tile face lists), so, unlike
+    Solver.autotune, each candidate is a handle of its own: set up, given
+    the cases' initial primitives `prims[i] = (rho, u, v, p)`, warmed up for
+    one CUDA graph, timed over `steps` steps (device time, CUDA events) and
+    destroyed before the next.  Returns the fastest candidate's make_launch
+    keywords (ready for setupSolver / Solver, and for Solver.autotune to
+    tune the rest on the chosen layout) and every trial's ms per step."""
+    trials = []
+    best = None
+    for order in orders:
+        for block in blocks:
+            kw = dict(launch_kw, order=order, block=block)
+            s = Solver(meshes, cfgs, make_launch(**kw))
+            try:
+                for i, p in enumerate(prims):
+                    s.createFields2d(i, *p)
+                s.propagate2d(max(32, launch_kw.get("graph_steps", 0) or 32))
+                s.propagate2d(steps)
+                total, cell, _ = s.last_timing()
+            finally:
+                s.close()
+            rec = {"order": order, "block": block, "ms_per_step": total / steps, "cell_kernel_ms": cell}
+            trials.append(rec)
+            if best is None or rec["ms_per_step"] < best[1]:
+                best = (kw, rec["ms_per_step"])
+    return best[0], trials
+
+
 def setupSolver(meshes, cfgs, **launch_kw) -> Solver:
     """setupSolver_*.jl + device setup for one or more cases."""
     if isinstance(meshes, Mesh2d):

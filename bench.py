@@ -345,11 +345,14 @@ def batched_mixed(pkg, items, s64, args, peak, kind):
     meshes = [m for m, _, _ in items]
     cfgs = [c for _, c, _ in items]
     cells = sum(m.nCells for m in meshes)
-    sm = pkg.solver.Solver(meshes, cfgs, pkg.solver.make_launch(precision="mixed", order=args.order, loop=args.loop,
-                                                                device=args.device, graph_steps=100))
+    # ordering and tile size first (each a handle of its own), then the
+    # launch shape on the chosen layout; the step loop is a 100-step graph
+    kw, layout_trials = pkg.solver.autotune_layout(meshes, cfgs, [p for _, _, p in items], precision="mixed",
+                                                   loop=args.loop, device=args.device, graph_steps=100)
+    sm = pkg.solver.Solver(meshes, cfgs, pkg.solver.make_launch(**kw))
     for i, (_, _, p) in enumerate(items):
         sm.createFields2d(i, *p)
-    tuned = sm.autotune(64)
+    tuned = dict(sm.autotune(64), order=kw["order"], block=kw["block"])
     sm.propagate2d(args.gpu_warmup)
     sm.propagate2d(args.steps)
     tot, cell_ms, launches = sm.last_timing()
@@ -412,6 +415,7 @@ def batched_mixed(pkg, items, s64, args, peak, kind):
     achieved = calg * cells / (cell_ms / 1e3) / 1e9 if cell_ms else None
     return {"value": value, "unit": "Mcell-steps/s", "cells": cells, "ms_per_step": tot / args.steps,
             "cell_kernel_ms": cell_ms, "gpu_launches": int(launches), "autotuned_launch": tuned,
+            "layout_trials": layout_trials,
             "roofline": {"achieved": achieved, "peak": peak, "frac": achieved / peak if achieved else None,
                          "alg_bytes_per_cell": calg, "step_alg_bytes_per_cell": alg,
                          "step_achieved_gbs": alg * cells / (tot / args.steps / 1e3) / 1e9},

@@ -89,6 +89,26 @@ def test_autotune_keeps_a_set_graph_length(pkg):
     s.close()
 
 
+def test_autotune_layout_picks_a_timed_candidate(pkg):
+    """Ordering and tile size are chosen among timed handles of their own;
+    the chosen layout steps to the same FP64 state as any other (results do
+    not depend on the layout)."""
+    mesh, cfg, prims = _viscous_case(pkg)
+    kw, trials = pkg.solver.autotune_layout([mesh], [cfg], [prims], orders=("hilbert", "natural"),
+                                            blocks=(256, 128), steps=16)
+    assert len(trials) == 4 and all(t["ms_per_step"] > 0.0 for t in trials)
+    best = min(trials, key=lambda t: t["ms_per_step"])
+    assert (kw["order"], kw["block"]) == (best["order"], best["block"])
+    out = []
+    for launch in (kw, {"order": "natural", "block": 256}):
+        s = pkg.setupSolver(mesh, cfg, **launch)
+        s.createFields2d(0, *prims)
+        s.propagate2d(12)
+        out.append(s.get_state(0)["Ucons"])
+        s.close()
+    assert np.array_equal(out[0], out[1])
+
+
 def test_autotune_needs_state(pkg):
     mesh, cfg, prims = _viscous_case(pkg)
     s = pkg.setupSolver(mesh, cfg)
