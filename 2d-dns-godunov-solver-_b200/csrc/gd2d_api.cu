@@ -922,6 +922,15 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     ALLOC(s.gpart, (size_t)ngroups * kPartials);
     ALLOC(s.group_done, ngroups);
     {
+        std::vector<int32_t> group_case((size_t)ngroups, 0);
+        for (int c = 0; c < n_cases; ++c)
+            for (int64_t gi = h->hcases[c].group_begin; gi < h->hcases[c].group_end; ++gi) group_case[gi] = c;
+        int32_t *d_gc;
+        ALLOC(d_gc, group_case.size()); UPLOAD(d_gc, group_case);
+        m.group_case = d_gc;
+        m.ngroups = ngroups;
+    }
+    {
         std::vector<int32_t> perm(Nc, 0), inv(NcRef, 0), ninv(NnRef, 0);
         int64_t maxrows = 1;
         for (const HostCase &hc : h->cases) {
@@ -1098,6 +1107,7 @@ static int init_case(gd2d_handle *h, int32_t icase, double t0, bool nodes_from_c
         CUDA_TRY(h, launch_init_state_mixed(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
         if (exact_cons)
             CUDA_TRY(h, launch_cols_to_dev(exact_cons, h->d_perm + hc.cell_off, hc.nc, h->s.U + hc.cell_off, h->stream));
+        CUDA_TRY(h, launch_reduce_groups(h->m, h->s, d.group_begin, d.group_end, true, h->stream));
         CUDA_TRY(h, launch_node_avg_mixed(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off,
                                           hc.node_off + hc.nn, h->lc, h->stream));
     } else {
@@ -1148,7 +1158,8 @@ int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, do
 }
 
 static int64_t kernels_per_step(const gd2d_handle *h) {
-    int64_t n = (h->visc ? 2 : 0) + 1;  // viscous gradient passes, node pass
+    // viscous gradient passes, group reduction (mixed), node pass
+    int64_t n = (h->visc ? 2 : 0) + (h->mixed ? 2 : 1);
     if (h->loop == GD2D_LOOP_FACE_COLOURED) n += (int64_t)h->colour_off.size() - 1 + 1;
     else if (h->loop == GD2D_LOOP_FACE_SLOTS) n += 2;
     else n += 1;
@@ -1194,6 +1205,12 @@ static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, 
     }
     if (e != cudaSuccess) return e;
     if (after_cell) record_timing(h, after_cell, in_capture);
+    // the mixed kernels' step reductions complete in a kernel of their own
+    // (the FP64 kernels reduce at each tile's end), then the node pass
+    if (h->mixed) {
+        e = launch_reduce_groups(h->m, h->s, 0, h->ngroups, false, h->stream);
+        if (e != cudaSuccess) return e;
+    }
     return h->mixed ? launch_node_avg_mixed(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream)
                     : launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream);
 }

@@ -95,6 +95,8 @@ struct DevMesh {
     const int32_t *cl;                   // [cluster_w][Nn], -1 = empty
     const double *wt;                    // [cluster_w][Nn] (NULL if unit weights)
     const int32_t *tile_case;            // [ntiles]
+    const int32_t *group_case;           // [ngroups] case of each tile group of the step reduction
+    int64_t ngroups;
     const int32_t *node_case;            // [Nn] (viscous only)
     const DevCase *cases;
     // mixed precision: FP32 copies of the geometry (the FP64 planes are not allocated)
@@ -144,7 +146,7 @@ struct DevState {
     NodeGrad *nodeG;   // [Nn] (viscous)
     double *part;      // [ntiles][kPartials]
     double *gpart;     // [ngroups][kPartials] group records
-    unsigned int *group_done;  // [ngroups] tiles of the group finished this step
+    unsigned int *group_done;  // [ngroups] warps of the group's tiles finished this step (FP64 kernels)
     CaseState *cstate; // [ncases]
     DevStats *ring;    // [ring_len][ncases]
     DevStats *ring_host;  // the host's page-locked, mapped copy of ring, written alongside it
@@ -206,6 +208,12 @@ cudaError_t launch_dev_to_cols(const double4 *src, const int32_t *inv, int64_t n
 cudaError_t launch_dev_to_cols_f(const float4 *src, const int32_t *inv, int64_t n, double *cols, cudaStream_t st);
 cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, bool flip_parity,
                                 bool zero_prims, int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st);
+// The step's two-level reduction of the tile records of groups [g0, g1)
+// after a mixed-precision cell kernel or state initialisation (the FP64
+// kernels reduce at each tile's end); the last group of each case finalizes
+// the case: statistics, flowTime, the next dt.
+cudaError_t launch_reduce_groups(const DevMesh &m, const DevState &s, int64_t g0, int64_t g1, bool is_init,
+                                 cudaStream_t st);
 cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,
                                   cudaStream_t st);

@@ -56,6 +56,12 @@ cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, 
     return launch_dependent(k_node_avg<false, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
 }
 
+cudaError_t launch_reduce_groups(const DevMesh &m, const DevState &s, int64_t g0, int64_t g1, bool is_init,
+                                 cudaStream_t st) {
+    if (g1 <= g0) return cudaSuccess;
+    return launch_dependent(k_reduce_groups, (int)(g1 - g0), 256, st, m, s, g0, is_init ? 1 : 0);
+}
+
 cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {
     const int b = lc.node_block;
     cudaError_t e = (m.nfmax == 4) ? launch_dependent(k_grad1_cells<true>, grid_for(m.Nc, b), b, st, m, s)

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
             if (VISC) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update_mixed(m, s, P, g, me, F, diff, dt, load_cell_in_f(m, s, g), pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, s_red, false);
+        tile_record(s, tile, part, s_red);
     }
 }
 
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(256) k_init_state_mixed(const DevMesh m, const
             part.vmax = vmax;
             part.rmin = (double)m.charlenf[g] / vmax;
         }
-        tile_epilogue(m, s, tile, c, part, s_red, true);
+        tile_record(s, tile, part, s_red);
     }
 }
 

@@ -238,6 +238,83 @@ __device__ __forceinline__ void tile_epilogue(const DevMesh &m, const DevState &
     __syncthreads();
 }
 
+// The mixed-precision kernels' tile record.  Every thread's Part goes to shared memory in
+// a transposed layout (`red`: kPartFields x blockDim doubles; it may alias
+// buffers the block used for the tile, the first barrier retires them).
+// Warp w reduces fields w, w + nwarps, ... (each lane folds its column in a
+// fixed order, then a fixed shuffle tree) and writes them into the tile's
+// record in global memory.  Nothing more happens at the tile's end: a
+// kernel of its own reduces the records after the cell kernel
+// (k_reduce_groups), so no tile waits for a fence or an atomic.  The
+// last barrier retires `red` for the next tile of a persistent block.
+__device__ __forceinline__ void tile_record(const DevState &s, int64_t tile, const Part &p, double *red) {
+    const int B = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = B >> 5;
+    __syncthreads();
+    p.store_strided(red + t, B);
+    __syncthreads();
+    double *rec = s.part + tile * kPartials;
+    for (int f = warp; f < kPartFields; f += nw) {
+        const double *row = red + f * B;
+        double x = row[lane];
+        for (int j = lane + 32; j < B; j += 32) x = part_op(f, x, row[j]);
+        for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
+        if (lane == 0) rec[f] = x;  // field f is record slot f
+    }
+    __syncthreads();
+}
+
+// The step's two-level reduction over the tile records the cell kernel
+// wrote (visible here: pdl_wait has returned), one block per group of
+// kGroupTiles tiles: each thread loads one tile record, the block folds the
+// records field by field in a fixed order (the transposed layout of
+// tile_record), and thread 0 stores the group record, fences it and counts
+// the group done for its case; the warp that completes a case's last group
+// reduces the case's group records and finalizes the case (finalize_case).
+// No thread waits on another's atomic; whichever block does a reduction, its
+// order is the same, so the results are deterministic.
+static __global__ void __launch_bounds__(256) k_reduce_groups(const DevMesh m, const DevState s, int64_t g0, int is_init) {
+    __shared__ double s_red[kPartFields * 256];
+    __shared__ double s_fields[kPartFields];
+    __shared__ int s_last;
+    pdl_trigger();
+    pdl_wait();
+    const int64_t gid = g0 + blockIdx.x;
+    const int c = m.group_case[gid];
+    const DevCase &P = m.cases[c];
+    const int64_t t0 = P.tile_begin + (gid - P.group_begin) * kGroupTiles;
+    const int64_t t1 = (t0 + kGroupTiles < P.tile_end) ? t0 + kGroupTiles : P.tile_end;
+    const int B = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = B >> 5;
+    Part p;
+    p.init();
+    for (int64_t q = t0 + t; q < t1; q += B) {
+        Part o;
+        o.load_cg(s.part + q * kPartials);
+        p.combine(o);
+    }
+    p.store_strided(s_red + t, B);
+    __syncthreads();
+    for (int f = warp; f < kPartFields; f += nw) {
+        const double *row = s_red + f * B;
+        double x = row[lane];
+        for (int j = lane + 32; j < B; j += 32) x = part_op(f, x, row[j]);
+        for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
+        if (lane == 0) s_fields[f] = x;
+    }
+    __syncthreads();
+    if (t == 0) {
+        double *g = s.gpart + gid * kPartials;
+        for (int f = 0; f < kPartFields; ++f) g[f] = s_fields[f];  // field f is record slot f
+        __threadfence();
+        const unsigned int ng = (unsigned int)(P.group_end - P.group_begin);
+        s_last = (atomicAdd(&s.cstate[c].tiles_done, 1u) == ng - 1u) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last && warp == 0) {
+        __threadfence();
+        finalize_case(m, s, c, is_init != 0);
+    }
+}
+
 // --------------------------------------------------------- MUSCL + flux
 
 // computeInterfaceSlope, computeslope2d.jl:3-136, for face k of cell g with
