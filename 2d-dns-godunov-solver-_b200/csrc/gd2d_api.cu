@@ -920,7 +920,6 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     ALLOC(s.parity, 1);
     ALLOC(s.node_done, 1);
     ALLOC(s.gpart, (size_t)ngroups * kPartials);
-    ALLOC(s.group_done, ngroups);
     {
         std::vector<int32_t> group_case((size_t)ngroups, 0);
         for (int c = 0; c < n_cases; ++c)
@@ -1107,15 +1106,16 @@ static int init_case(gd2d_handle *h, int32_t icase, double t0, bool nodes_from_c
         CUDA_TRY(h, launch_init_state_mixed(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
         if (exact_cons)
             CUDA_TRY(h, launch_cols_to_dev(exact_cons, h->d_perm + hc.cell_off, hc.nc, h->s.U + hc.cell_off, h->stream));
-        CUDA_TRY(h, launch_reduce_groups(h->m, h->s, d.group_begin, d.group_end, true, h->stream));
         CUDA_TRY(h, launch_node_avg_mixed(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off,
-                                          hc.node_off + hc.nn, h->lc, h->stream));
+                                          hc.node_off + hc.nn, d.group_begin, d.group_end, true, h->lc,
+                                          h->stream));
     } else {
         CUDA_TRY(h, launch_init_state_f64(h->m, h->s, d.tile_begin, d.tile_end, h->lc, h->stream));
         if (exact_cons)
             CUDA_TRY(h, launch_cols_to_dev(exact_cons, h->d_perm + hc.cell_off, hc.nc, h->s.U + hc.cell_off, h->stream));
         CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, !nodes_from_cells, hc.node_off,
-                                        hc.node_off + hc.nn, h->lc, h->stream));
+                                        hc.node_off + hc.nn, d.group_begin, d.group_end, true, h->lc,
+                                        h->stream));
     }
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     hc.state_set = true;
@@ -1158,8 +1158,8 @@ int gd2d_set_conservative(gd2d_handle *h, int32_t icase, const double *ucons, do
 }
 
 static int64_t kernels_per_step(const gd2d_handle *h) {
-    // viscous gradient passes, group reduction (mixed), node pass
-    int64_t n = (h->visc ? 2 : 0) + (h->mixed ? 2 : 1);
+    // viscous gradient passes, node pass (with the group reduction)
+    int64_t n = (h->visc ? 2 : 0) + 1;
     if (h->loop == GD2D_LOOP_FACE_COLOURED) n += (int64_t)h->colour_off.size() - 1 + 1;
     else if (h->loop == GD2D_LOOP_FACE_SLOTS) n += 2;
     else n += 1;
@@ -1205,14 +1205,12 @@ static cudaError_t launch_step_kernels(gd2d_handle *h, cudaEvent_t before_cell, 
     }
     if (e != cudaSuccess) return e;
     if (after_cell) record_timing(h, after_cell, in_capture);
-    // the mixed kernels' step reductions complete in a kernel of their own
-    // (the FP64 kernels reduce at each tile's end), then the node pass
-    if (h->mixed) {
-        e = launch_reduce_groups(h->m, h->s, 0, h->ngroups, false, h->stream);
-        if (e != cudaSuccess) return e;
-    }
-    return h->mixed ? launch_node_avg_mixed(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream)
-                    : launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, h->lc, h->stream);
+    // the node pass; its first blocks complete the step reduction of the
+    // cell kernel's tile records
+    return h->mixed ? launch_node_avg_mixed(h->m, h->s, h->visc, true, false, 0, h->m.Nn, 0, h->ngroups, false,
+                                            h->lc, h->stream)
+                    : launch_node_avg_f64(h->m, h->s, h->visc, true, false, 0, h->m.Nn, 0, h->ngroups, false,
+                                          h->lc, h->stream);
 }
 
 // Ends the capture opened on the handle's stream in every case (a stream
@@ -1453,7 +1451,7 @@ int gd2d_cells_to_nodes(gd2d_handle *h) {
     int rc = split_buffers(h);
     if (rc) return rc;
     cudaSetDevice(h->device);
-    CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, false, 0, h->m.Nn, h->lc, h->stream));
+    CUDA_TRY(h, launch_node_avg_f64(h->m, h->s, h->visc, false, false, 0, h->m.Nn, 0, 0, false, h->lc, h->stream));
     CUDA_TRY(h, cudaStreamSynchronize(h->stream));
     return GD2D_OK;
 }
@@ -1504,7 +1502,6 @@ std::vector<Region> step_state(const gd2d_handle *h) {
     add(s.parity, sizeof(int32_t));
     add(s.node_done, sizeof(unsigned int));
     add(s.gpart, sizeof(double) * h->ngroups * kPartials);
-    add(s.group_done, sizeof(unsigned int) * h->ngroups);
     add(h->Facc, sizeof(double4) * m.Nc);
     add(h->Fslot, sizeof(double4) * m.nfmax * m.Nc);
     return r;

@@ -59,7 +59,7 @@ struct DevCase {
 struct CaseState {
     double t, dt, velmax, rmin;
     int64_t step;
-    unsigned int tiles_done;  // tile groups of the case finished this step
+    unsigned int tiles_done;  // (tile group, record field) pairs of the case folded this step
     int32_t nonfinite;
 };
 
@@ -144,9 +144,8 @@ struct DevState {
     double4 *nodeC;    // [Nn] (viscous)
     NodeGrad *g1;      // [Nc] (viscous) first gradients per cell
     NodeGrad *nodeG;   // [Nn] (viscous)
-    double *part;      // [ntiles][kPartials]
+    double *part;      // tile records (FP64: field f of tile q at [f * ntiles + q]; mixed: [q * kPartials + f])
     double *gpart;     // [ngroups][kPartials] group records
-    unsigned int *group_done;  // [ngroups] warps of the group's tiles finished this step (FP64 kernels)
     CaseState *cstate; // [ncases]
     DevStats *ring;    // [ring_len][ncases]
     DevStats *ring_host;  // the host's page-locked, mapped copy of ring, written alongside it
@@ -206,14 +205,13 @@ cudaError_t launch_cons_to_prims(const double *cols, const int32_t *perm, int64_
                                  cudaStream_t st);
 cudaError_t launch_dev_to_cols(const double4 *src, const int32_t *inv, int64_t n, double *cols, cudaStream_t st);
 cudaError_t launch_dev_to_cols_f(const float4 *src, const int32_t *inv, int64_t n, double *cols, cudaStream_t st);
+// Node pass over nodes [n0, n1).  Its first blocks also complete the step
+// reduction of the tile records of groups [g0, g1) that the cell kernel (or
+// the state initialisation, red_init) wrote: the last group of each case
+// finalizes the case (statistics, flowTime, the next dt).  g0 == g1: none.
 cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, bool flip_parity,
-                                bool zero_prims, int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st);
-// The step's two-level reduction of the tile records of groups [g0, g1)
-// after a mixed-precision cell kernel or state initialisation (the FP64
-// kernels reduce at each tile's end); the last group of each case finalizes
-// the case: statistics, flowTime, the next dt.
-cudaError_t launch_reduce_groups(const DevMesh &m, const DevState &s, int64_t g0, int64_t g1, bool is_init,
-                                 cudaStream_t st);
+                                bool zero_prims, int64_t n0, int64_t n1, int64_t g0, int64_t g1, bool red_init,
+                                const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_init_state_f64(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1, const LaunchCfg &lc,
                                   cudaStream_t st);
@@ -242,7 +240,8 @@ cudaError_t launch_cell_step_mixed(const DevMesh &m, const DevState &s, int flux
 cudaError_t launch_cell_step_tf_mixed(const DevMesh &m, const DevState &s, int flux, bool visc, bool quads,
                                       const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_node_avg_mixed(const DevMesh &m, const DevState &s, bool visc, bool flip_parity,
-                                  bool zero_prims, int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st);
+                                  bool zero_prims, int64_t n0, int64_t n1, int64_t g0, int64_t g1, bool red_init,
+                                  const LaunchCfg &lc, cudaStream_t st);
 cudaError_t launch_visc_grad_mixed(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st);
 // U holds the case's FP64 primitives on entry and its conservatives on exit.
 cudaError_t launch_init_state_mixed(const DevMesh &m, const DevState &s, int64_t t0, int64_t t1,

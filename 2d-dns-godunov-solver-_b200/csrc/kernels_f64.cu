@@ -44,22 +44,19 @@ cudaError_t launch_cell_step_f64(const DevMesh &m, const DevState &s, int flux, 
 }
 
 cudaError_t launch_node_avg_f64(const DevMesh &m, const DevState &s, bool visc, bool flip_parity, bool zero_prims,
-                                int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st) {
+                                int64_t n0, int64_t n1, int64_t g0, int64_t g1, bool red_init, const LaunchCfg &lc,
+                                cudaStream_t st) {
     const int b = lc.node_block;
-    const int grid = grid_for(n1 - n0, b);
+    const int nred = (int)(g1 > g0 ? g1 - g0 : 0) * fold_blocks_per_group(b);
+    const int grid = grid_for(n1 - n0, b) + nred;
     const bool unit = m.unit_weights != 0;
+    const int fl = (int)flip_parity, zp = (int)zero_prims, ri = (int)red_init;
     if (visc) {
-        if (unit) return launch_dependent(k_node_avg<true, true>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
-        return launch_dependent(k_node_avg<true, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
+        if (unit) return launch_dependent(k_node_avg<true, true>, grid, b, st, m, s, fl, zp, n0, n1, g0, nred, ri);
+        return launch_dependent(k_node_avg<true, false>, grid, b, st, m, s, fl, zp, n0, n1, g0, nred, ri);
     }
-    if (unit) return launch_dependent(k_node_avg<false, true>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
-    return launch_dependent(k_node_avg<false, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
-}
-
-cudaError_t launch_reduce_groups(const DevMesh &m, const DevState &s, int64_t g0, int64_t g1, bool is_init,
-                                 cudaStream_t st) {
-    if (g1 <= g0) return cudaSuccess;
-    return launch_dependent(k_reduce_groups, (int)(g1 - g0), 256, st, m, s, g0, is_init ? 1 : 0);
+    if (unit) return launch_dependent(k_node_avg<false, true>, grid, b, st, m, s, fl, zp, n0, n1, g0, nred, ri);
+    return launch_dependent(k_node_avg<false, false>, grid, b, st, m, s, fl, zp, n0, n1, g0, nred, ri);
 }
 
 cudaError_t launch_visc_grad_f64(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
             if (VISC) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update_mixed(m, s, P, g, me, F, diff, dt, load_cell_in_f(m, s, g), pout, part);
         }
-        tile_record(s, tile, part, s_red);
+        tile_record<false>(m, s, tile, part, s_red);
     }
 }
 
@@ -88,13 +88,18 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
 // resident blocks per SM.
 template <bool VISC, bool UNIT>
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_node_avg_mixed(const DevMesh m, const DevState s, int flip, int zero_prims,
-                                                        int64_t n0, int64_t n1) {
+                                                        int64_t n0, int64_t n1, int64_t g0, int nred, int is_init) {
     pdl_trigger();
     pdl_wait();
+    if ((int)blockIdx.x < nred) {
+        fold_block<false>(m, s, g0, is_init != 0);
+        return;
+    }
+    const int64_t bid = (int64_t)blockIdx.x - nred, nblk = (int64_t)gridDim.x - nred;
     const int par = *s.parity;
     const float4 *__restrict__ src = s.primf + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
     const int W = m.cluster_w;
-    for (int64_t J = n0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < n1; J += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t J = n0 + bid * blockDim.x + threadIdx.x; J < n1; J += nblk * blockDim.x) {
         bool prim_form = false;
         float gop = 0.f, gam = 0.f;
         if (VISC) {
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_node_avg_mixed(co
         // this kernel reads what the others wrote, so no fence: stream order
         // makes the flip and the node values visible to the next kernel.
         __syncthreads();
-        if (threadIdx.x == 0 && atomicAdd(s.node_done, 1u) == gridDim.x - 1u) {
+        if (threadIdx.x == 0 && atomicAdd(s.node_done, 1u) == (unsigned int)nblk - 1u) {
             *s.node_done = 0u;
             *s.parity = par ^ 1;
         }
@@ -242,7 +247,7 @@ __global__ void __launch_bounds__(256) k_init_state_mixed(const DevMesh m, const
             part.vmax = vmax;
             part.rmin = (double)m.charlenf[g] / vmax;
         }
-        tile_record(s, tile, part, s_red);
+        tile_record<false>(m, s, tile, part, s_red);
     }
 }
 
@@ -281,16 +286,19 @@ cudaError_t launch_cell_step_mixed(const DevMesh &m, const DevState &s, int flux
 }
 
 cudaError_t launch_node_avg_mixed(const DevMesh &m, const DevState &s, bool visc, bool flip_parity, bool zero_prims,
-                                  int64_t n0, int64_t n1, const LaunchCfg &lc, cudaStream_t st) {
+                                  int64_t n0, int64_t n1, int64_t g0, int64_t g1, bool red_init, const LaunchCfg &lc,
+                                  cudaStream_t st) {
     const int b = lc.node_block;
-    const int grid = grid_for_m(n1 - n0, b);
+    const int nred = (int)(g1 > g0 ? g1 - g0 : 0) * fold_blocks_per_group(b);
+    const int grid = grid_for_m(n1 - n0, b) + nred;
     const bool unit = m.unit_weights != 0;
+    const int fl = (int)flip_parity, zp = (int)zero_prims, ri = (int)red_init;
     if (visc) {
-        if (unit) return launch_dependent(k_node_avg_mixed<true, true>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
-        return launch_dependent(k_node_avg_mixed<true, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
+        if (unit) return launch_dependent(k_node_avg_mixed<true, true>, grid, b, st, m, s, fl, zp, n0, n1, g0, nred, ri);
+        return launch_dependent(k_node_avg_mixed<true, false>, grid, b, st, m, s, fl, zp, n0, n1, g0, nred, ri);
     }
-    if (unit) return launch_dependent(k_node_avg_mixed<false, true>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
-    return launch_dependent(k_node_avg_mixed<false, false>, grid, b, st, m, s, (int)flip_parity, (int)zero_prims, n0, n1);
+    if (unit) return launch_dependent(k_node_avg_mixed<false, true>, grid, b, st, m, s, fl, zp, n0, n1, g0, nred, ri);
+    return launch_dependent(k_node_avg_mixed<false, false>, grid, b, st, m, s, fl, zp, n0, n1, g0, nred, ri);
 }
 
 cudaError_t launch_visc_grad_mixed(const DevMesh &m, const DevState &s, const LaunchCfg &lc, cudaStream_t st) {

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
             }
             cell_update_mixed(m, s, P, g, me, F, diff, dt, cin, pout, part);
         }
-        tile_record(s, tile, part, s_red);
+        tile_record<false>(m, s, tile, part, s_red);
     }
 }
 

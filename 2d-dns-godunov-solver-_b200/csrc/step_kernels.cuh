@@ -142,7 +142,7 @@ __device__ __forceinline__ Part warp_reduce_records(const double *recs, int64_t 
 // and the next dt: the fixed solControls.dt the reference steps with, or
 // opt-in, the tau it reports (testInviscidFluxesGPUx32.jl:299,324) or the
 // local-CFL extension.
-static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c, bool is_init) {
+static __device__ __forceinline__ void finalize_case(const DevMesh &m, const DevState &s, int c, bool is_init) {
     const DevCase &P = m.cases[c];
     const Part acc = warp_reduce_records(s.gpart, P.group_begin, P.group_end);
     if ((threadIdx.x & 31) == 0) {
@@ -179,140 +179,105 @@ static __device__ void finalize_case(const DevMesh &m, const DevState &s, int c,
     }
 }
 
-// The tile's reduction record and the step's two-level completion count.
-//
-// Every thread's Part goes to shared memory in a transposed layout (`red`:
-// kPartFields x blockDim doubles; it may alias buffers the block used for
-// the tile, the first barrier retires them).  Warp w reduces fields w, w +
-// nwarps, ... (each lane folds its column in a fixed order, then a fixed
-// shuffle tree), writes them into the tile's record in global memory, and
-// counts itself done for the tile's group.  The warp that completes a group
-// of kGroupTiles tiles reduces the group's records into a group record; the
-// warp that completes a case's last group finalizes the case.  No thread
-// waits on another's atomic; whichever warp ends up doing a reduction, its
-// order is the same, so the results are deterministic.
-__device__ __forceinline__ void tile_epilogue(const DevMesh &m, const DevState &s, int64_t tile, int c, Part &p,
-                                              double *red, bool is_init) {
-    const DevCase &P = m.cases[c];
+// Field f of tile q's reduction record.  Two layouts, measured per
+// precision on the 2.09M-cell viscous cylinder: FIELD_MAJOR (one row of
+// ntiles doubles per field), which makes the FP64 cell kernel 10 us faster
+// than records of kPartials doubles and the mixed one 6 us slower, so the
+// FP64 kernels use it and the mixed kernels do not.  The layout is a
+// template parameter: strides read at run time cost the mixed cell kernel
+// spills and 4 us.
+template <bool FIELD_MAJOR>
+__device__ __forceinline__ double *part_at(const DevMesh &m, const DevState &s, int64_t q, int f) {
+    return FIELD_MAJOR ? s.part + (int64_t)f * m.ntiles + q : s.part + q * kPartials + f;
+}
+
+// The tile's reduction record.  Every thread's Part goes to shared memory
+// in a transposed layout (`red`: kPartFields x blockDim doubles; it may
+// alias buffers the block used for the tile, the first barrier retires
+// them).  Warp w reduces fields w, w + nwarps, ... (each lane folds its
+// column in a fixed order, then a fixed shuffle tree) and writes them into
+// the tile's record.  Nothing more happens at the tile's end: the next node
+// pass folds the records (fold_field), so no tile waits for a fence or an
+// atomic.  The last barrier retires `red` for the next tile of a
+// persistent block.
+template <bool FIELD_MAJOR>
+__device__ __forceinline__ void tile_record(const DevMesh &m, const DevState &s, int64_t tile, const Part &p,
+                                            double *red) {
     const int B = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = B >> 5;
-    const int64_t gi = (tile - P.tile_begin) / kGroupTiles;
-    const int64_t gid = P.group_begin + gi;
-    const int64_t t0 = P.tile_begin + gi * kGroupTiles;
-    const int64_t t1 = (t0 + kGroupTiles < P.tile_end) ? t0 + kGroupTiles : P.tile_end;
     __syncthreads();
     p.store_strided(red + t, B);
     __syncthreads();
-    double *rec = s.part + tile * kPartials;
     for (int f = warp; f < kPartFields; f += nw) {
         const double *row = red + f * B;
         double x = row[lane];
         for (int j = lane + 32; j < B; j += 32) x = part_op(f, x, row[j]);
         for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
-        if (lane == 0) rec[f] = x;  // field f is record slot f
+        if (lane == 0) *part_at<FIELD_MAJOR>(m, s, tile, f) = x;
     }
+    __syncthreads();
+}
+
+// Identity of field f of a Part (record order), as Part::init sets it.
+__device__ __forceinline__ double part_ident(int f) {
+    if (f == 10 || f == 11) return INFINITY;
+    return f == 12 ? -INFINITY : 0.0;
+}
+
+// Blocks of a node pass that fold one tile group: one warp per (group,
+// field) pair, so a group takes kPartFields / warps-per-block blocks.
+__host__ __device__ __forceinline__ int fold_blocks_per_group(int block) {
+    const int nw = block / 32;
+    return (kPartFields + nw - 1) / nw;
+}
+
+// The step's two-level reduction, done by warps of the node pass that
+// follows the cell kernel (the cell kernel's tile records are visible
+// there: pdl_wait has returned).  One warp folds field f of tile group
+// `gid` (up to kGroupTiles tiles of one case) into the group's record: lane
+// l takes records l, l + 32, ..., l + kGroupTiles - 32 of the group in
+// turn, then a fixed shuffle tree over the lanes.  It then counts the field
+// done for the case; the warp that completes the case's last (group, field)
+// pair reduces the case's group records and finalizes the case
+// (finalize_case).  No thread waits on another's atomic; whichever warp
+// finalizes, the order of every sum is the same, so the results are
+// deterministic and do not depend on the node pass's block size.
+template <bool FIELD_MAJOR>
+static __device__ __forceinline__ void fold_field(const DevMesh &m, const DevState &s, int64_t gid, int f,
+                                               bool is_init) {
+    constexpr int kPerLane = kGroupTiles / 32;
+    const int c = m.group_case[gid];
+    const DevCase &P = m.cases[c];
+    const int64_t t0 = P.tile_begin + (gid - P.group_begin) * kGroupTiles;
+    const int n = (int)((t0 + kGroupTiles < P.tile_end) ? kGroupTiles : P.tile_end - t0);
+    const int lane = threadIdx.x & 31;
+    const double id = part_ident(f);
+    double v[kPerLane];
+#pragma unroll
+    for (int j = 0; j < kPerLane; ++j) v[j] = (lane + 32 * j < n) ? __ldcg(part_at<FIELD_MAJOR>(m, s, t0 + lane + 32 * j, f)) : id;
+    double x = v[0];
+#pragma unroll
+    for (int j = 1; j < kPerLane; ++j) x = part_op(f, x, v[j]);
+    for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
     int last = 0;
     if (lane == 0) {
+        s.gpart[gid * kPartials + f] = x;  // field f is record slot f
         __threadfence();
-        const unsigned int need = (unsigned int)((t1 - t0) * nw);
-        last = (atomicAdd(&s.group_done[gid], 1u) == need - 1u) ? 1 : 0;
+        const unsigned int need = (unsigned int)((P.group_end - P.group_begin) * kPartFields);
+        last = (atomicAdd(&s.cstate[c].tiles_done, 1u) == need - 1u) ? 1 : 0;
     }
     last = __shfl_sync(0xffffffffu, last, 0);
     if (last) {
         __threadfence();
-        const Part acc = warp_reduce_records(s.part, t0, t1);
-        int last_case = 0;
-        if (lane == 0) {
-            acc.store(s.gpart + gid * kPartials);
-            s.group_done[gid] = 0u;
-            __threadfence();
-            const unsigned int ng = (unsigned int)(P.group_end - P.group_begin);
-            last_case = (atomicAdd(&s.cstate[c].tiles_done, 1u) == ng - 1u) ? 1 : 0;
-        }
-        last_case = __shfl_sync(0xffffffffu, last_case, 0);
-        if (last_case) {
-            __threadfence();
-            finalize_case(m, s, c, is_init);
-        }
+        finalize_case(m, s, c, is_init);
     }
-    // the next tile may reuse what `red` aliases
-    __syncthreads();
 }
 
-// The mixed-precision kernels' tile record.  Every thread's Part goes to shared memory in
-// a transposed layout (`red`: kPartFields x blockDim doubles; it may alias
-// buffers the block used for the tile, the first barrier retires them).
-// Warp w reduces fields w, w + nwarps, ... (each lane folds its column in a
-// fixed order, then a fixed shuffle tree) and writes them into the tile's
-// record in global memory.  Nothing more happens at the tile's end: a
-// kernel of its own reduces the records after the cell kernel
-// (k_reduce_groups), so no tile waits for a fence or an atomic.  The
-// last barrier retires `red` for the next tile of a persistent block.
-__device__ __forceinline__ void tile_record(const DevState &s, int64_t tile, const Part &p, double *red) {
-    const int B = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = B >> 5;
-    __syncthreads();
-    p.store_strided(red + t, B);
-    __syncthreads();
-    double *rec = s.part + tile * kPartials;
-    for (int f = warp; f < kPartFields; f += nw) {
-        const double *row = red + f * B;
-        double x = row[lane];
-        for (int j = lane + 32; j < B; j += 32) x = part_op(f, x, row[j]);
-        for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
-        if (lane == 0) rec[f] = x;  // field f is record slot f
-    }
-    __syncthreads();
-}
-
-// The step's two-level reduction over the tile records the cell kernel
-// wrote (visible here: pdl_wait has returned), one block per group of
-// kGroupTiles tiles: each thread loads one tile record, the block folds the
-// records field by field in a fixed order (the transposed layout of
-// tile_record), and thread 0 stores the group record, fences it and counts
-// the group done for its case; the warp that completes a case's last group
-// reduces the case's group records and finalizes the case (finalize_case).
-// No thread waits on another's atomic; whichever block does a reduction, its
-// order is the same, so the results are deterministic.
-static __global__ void __launch_bounds__(256) k_reduce_groups(const DevMesh m, const DevState s, int64_t g0, int is_init) {
-    __shared__ double s_red[kPartFields * 256];
-    __shared__ double s_fields[kPartFields];
-    __shared__ int s_last;
-    pdl_trigger();
-    pdl_wait();
-    const int64_t gid = g0 + blockIdx.x;
-    const int c = m.group_case[gid];
-    const DevCase &P = m.cases[c];
-    const int64_t t0 = P.tile_begin + (gid - P.group_begin) * kGroupTiles;
-    const int64_t t1 = (t0 + kGroupTiles < P.tile_end) ? t0 + kGroupTiles : P.tile_end;
-    const int B = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = B >> 5;
-    Part p;
-    p.init();
-    for (int64_t q = t0 + t; q < t1; q += B) {
-        Part o;
-        o.load_cg(s.part + q * kPartials);
-        p.combine(o);
-    }
-    p.store_strided(s_red + t, B);
-    __syncthreads();
-    for (int f = warp; f < kPartFields; f += nw) {
-        const double *row = s_red + f * B;
-        double x = row[lane];
-        for (int j = lane + 32; j < B; j += 32) x = part_op(f, x, row[j]);
-        for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
-        if (lane == 0) s_fields[f] = x;
-    }
-    __syncthreads();
-    if (t == 0) {
-        double *g = s.gpart + gid * kPartials;
-        for (int f = 0; f < kPartFields; ++f) g[f] = s_fields[f];  // field f is record slot f
-        __threadfence();
-        const unsigned int ng = (unsigned int)(P.group_end - P.group_begin);
-        s_last = (atomicAdd(&s.cstate[c].tiles_done, 1u) == ng - 1u) ? 1 : 0;
-    }
-    __syncthreads();
-    if (s_last && warp == 0) {
-        __threadfence();
-        finalize_case(m, s, c, is_init != 0);
-    }
+// Block b < nred of a node pass: its warps fold (group, field) pairs.
+template <bool FIELD_MAJOR>
+__device__ __forceinline__ void fold_block(const DevMesh &m, const DevState &s, int64_t g0, bool is_init) {
+    const int bpg = fold_blocks_per_group(blockDim.x);
+    const int f = (int)(blockIdx.x % bpg) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (f < kPartFields) fold_field<FIELD_MAJOR>(m, s, g0 + blockIdx.x / bpg, f, is_init);
 }
 
 // --------------------------------------------------------- MUSCL + flux
@@ -549,7 +514,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const 
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update(m, s, P, g, me, F, diff, dt, load_cell_in(m, s, g), pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, s_red, false);
+        tile_record<true>(m, s, tile, part, s_red);
     }
 }
 
@@ -662,7 +627,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
             }
             cell_update(m, s, P, g, me, F, diff, dt, cin, pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, s_red, false);
+        tile_record<true>(m, s, tile, part, s_red);
     }
 }
 
@@ -671,19 +636,27 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
 // cells2nodesSolutionReconstructionWithStencils (utilsFVM2dp.jl:299-365):
 // weighted primitive averages; with VISC also calcPhiInCellCluster's
 // unweighted means of rho u, rho v, E (calcGradients.jl:3-18) for the next
-// step's viscous term.  The last block flips the step parity.
+// step's viscous term.  The last block flips the step parity.  The first
+// `nred` blocks instead fold the cell kernel's tile groups g0, g0 + 1, ...
+// (fold_block): they start first and their latency hides behind the node
+// gathers; nothing here reads what they write.
 // The node-side kernels are bound by the latency of their gathers; their
 // register budget is capped for 4 resident blocks per SM (more warps in
 // flight; measured faster than the unconstrained 76-register build).
 template <bool VISC, bool UNIT>
 __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_node_avg(const DevMesh m, const DevState s, int flip, int zero_prims,
-                                                  int64_t n0, int64_t n1) {
+                                                  int64_t n0, int64_t n1, int64_t g0, int nred, int is_init) {
     pdl_trigger();
     pdl_wait();
+    if ((int)blockIdx.x < nred) {
+        fold_block<true>(m, s, g0, is_init != 0);
+        return;
+    }
+    const int64_t bid = (int64_t)blockIdx.x - nred, nblk = (int64_t)gridDim.x - nred;
     const int par = *s.parity;
     const double4 *__restrict__ src = s.prim + (int64_t)(flip ? (par ^ 1) : par) * m.Nc;
     const int W = m.cluster_w;
-    for (int64_t J = n0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; J < n1; J += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t J = n0 + bid * blockDim.x + threadIdx.x; J < n1; J += nblk * blockDim.x) {
         bool prim_form = false;
         double gop = 0.0, gam = 0.0;
         if (VISC) {
@@ -739,7 +712,7 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB) k_node_avg(const DevMesh 
         // this kernel reads what the others wrote, so no fence: stream order
         // makes the flip and the node values visible to the next kernel.
         __syncthreads();
-        if (threadIdx.x == 0 && atomicAdd(s.node_done, 1u) == gridDim.x - 1u) {
+        if (threadIdx.x == 0 && atomicAdd(s.node_done, 1u) == (unsigned int)nblk - 1u) {
             *s.node_done = 0u;
             *s.parity = par ^ 1;
         }
@@ -857,7 +830,7 @@ static __global__ void __launch_bounds__(256) k_init_state(const DevMesh m, cons
             part.vmax = vmax;
             part.rmin = m.charlen[g] / vmax;
         }
-        tile_epilogue(m, s, tile, c, part, s_red, true);
+        tile_record<true>(m, s, tile, part, s_red);
     }
 }
 
@@ -948,7 +921,7 @@ __global__ void __launch_bounds__(256, MINB) k_face_update(const DevMesh m, cons
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update(m, s, P, g, me, F, diff, dt, load_cell_in(m, s, g), pout, part);
         }
-        tile_epilogue(m, s, tile, c, part, s_red, false);
+        tile_record<true>(m, s, tile, part, s_red);
     }
 }
 
