@@ -854,6 +854,19 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
         ALLOC(f_charlen, Nc); UPLOAD(f_charlen, to_f(charlen));
         m.nxf = f_nx; m.nyf = f_ny; m.lenf = f_len; m.rareaf = f_rarea; m.areaf = f_area; m.hxf = f_hx;
         m.charlenf = f_charlen;
+        if (h->visc) {
+            // the first gradient's edge weights, one plane each instead of
+            // three (normal components and length)
+            std::vector<float> nlx((size_t)nfmax * Nc), nly((size_t)nfmax * Nc);
+            for (size_t i = 0; i < nlx.size(); ++i) {
+                nlx[i] = (float)(gnx[i] * glen[i]);
+                nly[i] = (float)(gny[i] * glen[i]);
+            }
+            float *f_nlx, *f_nly;
+            ALLOC(f_nlx, nlx.size()); UPLOAD(f_nlx, nlx);
+            ALLOC(f_nly, nly.size()); UPLOAD(f_nly, nly);
+            m.nlxf = f_nlx; m.nlyf = f_nly;
+        }
     }
     if (h->tgv) {
         ALLOC(d_mid, Nc); UPLOAD(d_mid, mid);

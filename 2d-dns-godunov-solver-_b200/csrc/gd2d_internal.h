@@ -101,6 +101,7 @@ struct DevMesh {
     const DevCase *cases;
     // mixed precision: FP32 copies of the geometry (the FP64 planes are not allocated)
     const float *nxf, *nyf, *lenf;       // [nfmax][Nc]
+    const float *nlxf, *nlyf;            // [nfmax][Nc] (viscous) nx * len, ny * len, rounded once to FP32
     const float *rareaf, *areaf, *hxf, *charlenf;
     // tile-local face lists (GD2D_LOOP_TILE_FACES): faces of tile t are
     // [tf_off[t], tf_off[t+1]); tf_rec = (neighbour code, packed slots, dn, up)

@@ -161,30 +161,30 @@ __global__ void __launch_bounds__(256, GD2D_NODE_MINB_MIXED) k_grad1_cells_mixed
     pdl_wait();
     for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < m.Nc; g += (int64_t)gridDim.x * blockDim.x) {
         // all per-cell loads first (two trips to memory per cell); padding
-        // cells have zero area and are dropped at the store, triangles have
-        // a zero-length fourth edge
-        const float area = ld_once(m.areaf + g), rA = ld_once(m.rareaf + g);
-        float side[NF], nx[NF], ny[NF];
+        // cells have zero inverse area and are dropped at the store,
+        // triangles have a zero-length fourth edge; each edge's weights
+        // are n * len, rounded once
+        const float rA = ld_once(m.rareaf + g);
+        float nlx[NF], nly[NF];
         int2 e[NF];
 #pragma unroll
         for (int k = 0; k < NF; ++k) {
             const int64_t o = (int64_t)k * m.Nc + g;
-            side[k] = ld_once(m.lenf + o);
-            nx[k] = ld_once(m.nxf + o);
-            ny[k] = ld_once(m.nyf + o);
+            nlx[k] = ld_once(m.nlxf + o);
+            nly[k] = ld_once(m.nlyf + o);
             e[k] = ld_once(m.c2n + o);
         }
-        const int nf = (QUAD && side[NF - 1] != 0.f) ? 4 : 3;
+        const int nf = (QUAD && ld_once(m.lenf + (int64_t)(NF - 1) * m.Nc + g) != 0.f) ? 4 : 3;
         float sx[3] = {0.f, 0.f, 0.f}, sy[3] = {0.f, 0.f, 0.f};
 #pragma unroll
         for (int k = 0; k < NF; ++k) {
             if (k >= nf) break;
             const float4 A = s.nodeCf[e[k].x], B = s.nodeCf[e[k].y];
-            sx[0] += 0.5f * (A.x + B.x) * -ny[k] * side[k]; sy[0] += 0.5f * (A.x + B.x) * -nx[k] * side[k];
-            sx[1] += 0.5f * (A.y + B.y) * -ny[k] * side[k]; sy[1] += 0.5f * (A.y + B.y) * -nx[k] * side[k];
-            sx[2] += 0.5f * (A.z + B.z) * -ny[k] * side[k]; sy[2] += 0.5f * (A.z + B.z) * -nx[k] * side[k];
+            sx[0] += 0.5f * (A.x + B.x) * -nly[k]; sy[0] += 0.5f * (A.x + B.x) * -nlx[k];
+            sx[1] += 0.5f * (A.y + B.y) * -nly[k]; sy[1] += 0.5f * (A.y + B.y) * -nlx[k];
+            sx[2] += 0.5f * (A.z + B.z) * -nly[k]; sy[2] += 0.5f * (A.z + B.z) * -nlx[k];
         }
-        if (area == 0.f) continue;
+        if (rA == 0.f) continue;
         NodeGradF r;
         r.ru = make_float2(sx[0] * rA, sy[0] * rA);
         r.rv = make_float2(sx[1] * rA, sy[1] * rA);
