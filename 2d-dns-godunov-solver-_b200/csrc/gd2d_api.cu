@@ -435,11 +435,10 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
     }
     h->lc.persistent = h->launch.persistent;
     // register budget of the cell kernel, measured best on the 2.09M-cell
-    // viscous cylinder: 3 blocks/SM for the FP64 cell-centred kernel, 4 for
-    // the FP64 tile-face kernel and for the mixed kernels
-    h->lc.min_blocks = h->launch.min_blocks
-                           ? h->launch.min_blocks
-                           : ((h->mixed || h->launch.loop == GD2D_LOOP_TILE_FACES) ? 4 : 3);
+    // viscous cylinder: 3 blocks/SM for the FP64 kernels (the tile-face
+    // kernel holds its next face record through the current face), 4 for
+    // the mixed kernels
+    h->lc.min_blocks = h->launch.min_blocks ? h->launch.min_blocks : (h->mixed ? 4 : 3);
     if (h->lc.min_blocks < 2 || h->lc.min_blocks > 4) {
         delete h;
         return fail(nullptr, GD2D_ERR_ARG, "min_blocks must be 2, 3 or 4");

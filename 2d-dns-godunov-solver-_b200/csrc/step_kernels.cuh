@@ -559,11 +559,18 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
         const DevCase &P = m.cases[c];
         const double t = s.cstate[c].t;
         const bool venkat = P.limiter == LIM_VENKAT;
+        // face indices fit 32 bits (setup checks the total); the first face
+        // record goes out with the staging loads and each next one before
+        // the current face's gathers, so no face waits for its record
+        const int fb = (int)f0 + (int)threadIdx.x, fe = (int)f1;
+        int4 next = make_int4(0, 0, 0, 0);
+        if (fb < fe) next = ld_once(m.tf_rec + fb);
         __syncthreads();
         const double gam = P.gamma;
         const double g2 = 2.0 * (gam - 1.0) / (gam + 1.0);
-        for (int64_t f = f0 + threadIdx.x; f < f1; f += B) {
-            const int4 rec = ld_once(m.tf_rec + f);
+        for (int f = fb; f < fe; f += B) {
+            const int4 rec = next;
+            if (f + B < fe) next = ld_once(m.tf_rec + f + B);
             const TileFace tf = unpack_tile_face(rec.y);
             const double4 a4 = s_prim[tf.la];
             const double uL[4] = {a4.x, a4.y, a4.z, a4.w};
