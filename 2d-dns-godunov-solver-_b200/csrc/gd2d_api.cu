@@ -1023,8 +1023,29 @@ static void stage_copy(double *stage, double *const cols[4], int64_t n, size_t b
     }
 }
 
+// Whether a host buffer is page-locked in the current context (allocated
+// or registered with CUDA), so that the copy engine can read or write it
+// directly.  Pageable memory is not an error.
+static bool host_pinned(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 // Host columns -> h_stage -> d_stage (queued on the handle's stream).
+// Page-locked columns are copied to d_stage directly.
 static int staged_upload(gd2d_handle *h, const double *const src[4], int64_t n) {
+    if (host_pinned(src[0]) && host_pinned(src[1]) && host_pinned(src[2]) && host_pinned(src[3])) {
+        for (int v = 0; v < 4; ++v) {
+            const cudaError_t e = cudaMemcpyAsync(h->d_stage + (size_t)v * n, src[v], sizeof(double) * (size_t)n,
+                                                  cudaMemcpyHostToDevice, h->stream);
+            if (e != cudaSuccess) return fail(h, GD2D_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+        }
+        return GD2D_OK;
+    }
     double *cols[4] = {const_cast<double *>(src[0]), const_cast<double *>(src[1]), const_cast<double *>(src[2]),
                        const_cast<double *>(src[3])};
     const size_t total = 4 * (size_t)n;
@@ -1042,10 +1063,19 @@ static int staged_upload(gd2d_handle *h, const double *const src[4], int64_t n) 
 }
 
 // d_stage -> h_stage -> a column-major (n, 4) host matrix; returns when the
-// matrix is complete.
+// matrix is complete.  A page-locked matrix is copied to directly.
 static int staged_download(gd2d_handle *h, double *dst, int64_t n) {
-    double *cols[4] = {dst, dst + n, dst + 2 * n, dst + 3 * n};
     const size_t total = 4 * (size_t)n;
+    if (host_pinned(dst)) {
+        cudaError_t e = cudaMemcpyAsync(dst, h->d_stage, sizeof(double) * total, cudaMemcpyDeviceToHost, h->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) {
+            cudaStreamSynchronize(h->stream);
+            return fail(h, GD2D_ERR_CUDA, "download: %s", cudaGetErrorString(e));
+        }
+        return GD2D_OK;
+    }
+    double *cols[4] = {dst, dst + n, dst + 2 * n, dst + 3 * n};
     const unsigned ns = (unsigned)((total + kSliceElems - 1) / kSliceElems);
     cudaError_t e = cudaSuccess;
     while (e == cudaSuccess && h->slice_ev.size() < ns) {
