@@ -50,7 +50,7 @@ CELL_ALG_BYTES = {("f64", False): 180, ("f64", True): 212, ("mixed", False): 140
 # measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum of one
 # launch; FP64 cell-centred on 1025^2 nodes, the others on 513^2 nodes, the
 # traffic growing in proportion to the cells); None where not captured.
-CELL_KERNEL_TRAFFIC = {("f64", "cell"): 337.0, ("f64", "tile"): 292.0, ("mixed", "cell"): 233.0,
+CELL_KERNEL_TRAFFIC = {("f64", "cell"): 337.0, ("f64", "tile"): 282.0, ("mixed", "cell"): 233.0,
                        ("mixed", "tile"): 148.0}
 
 
