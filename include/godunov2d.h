@@ -169,7 +169,11 @@ int gd2d_setup(gd2d_handle **out, int32_t n_cases, const gd2d_mesh_view *meshes,
                const gd2d_params *params, const gd2d_launch *launch);
 
 /* createFields2d + phs2dcns2dcellsSA + the conservative node average
- * (initfields_*.jl createFields2d, utilsFVM2dp.jl:4-17, 370-422). */
+ * (initfields_*.jl createFields2d, utilsFVM2dp.jl:4-17, 370-422).
+ * Host arrays that are page-locked (cudaHostAlloc / cudaHostRegister, or
+ * pinned by the caller's CUDA binding) are copied to the device directly;
+ * pageable ones go through the library's own page-locked stage.  The same
+ * holds for every host array of gd2d_set_conservative and gd2d_get_state. */
 int gd2d_set_state(gd2d_handle *h, int32_t icase, const double *density, const double *ux,
                    const double *uy, const double *pressure);
 
