@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_mixed(const DevMesh m, 
             if (VISC) diff_source_f<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update_mixed(m, s, P, g, me, F, diff, dt, load_cell_in_f(m, s, g), pout, part);
         }
-        tile_record<false>(m, s, tile, part, s_red);
+        tile_record<false, false>(m, s, tile, part, s_red);
     }
 }
 
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(256) k_init_state_mixed(const DevMesh m, const
             part.vmax = vmax;
             part.rmin = (double)m.charlenf[g] / vmax;
         }
-        tile_record<false>(m, s, tile, part, s_red);
+        tile_record<false, false>(m, s, tile, part, s_red);
     }
 }
 

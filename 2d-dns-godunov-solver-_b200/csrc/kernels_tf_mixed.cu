@@ -32,7 +32,6 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
     constexpr int kBufBytes = kTileBytes > kRedBytes ? kTileBytes : kRedBytes;
     __shared__ double4 s_buf[kBufBytes / 32];
     __shared__ float s_hx[256];
-    double *const s_red = reinterpret_cast<double *>(s_buf);
     float4 *const s_prim = reinterpret_cast<float4 *>(s_buf);
     float4 (*const s_flux)[256] = reinterpret_cast<float4 (*)[256]>(s_prim + 256);
     float4 (*const s_visc)[256] = reinterpret_cast<float4 (*)[256]>(s_prim + 256 * (1 + NS));
@@ -156,7 +155,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf_mixed(const DevMesh 
             }
             cell_update_mixed(m, s, P, g, me, F, diff, dt, cin, pout, part);
         }
-        tile_record<false>(m, s, tile, part, s_red);
+        tile_record<false, true>(m, s, tile, part, reinterpret_cast<double *>(s_buf));
     }
 }
 

@@ -191,28 +191,44 @@ __device__ __forceinline__ double *part_at(const DevMesh &m, const DevState &s, 
     return FIELD_MAJOR ? s.part + (int64_t)f * m.ntiles + q : s.part + q * kPartials + f;
 }
 
-// The tile's reduction record.  Every thread's Part goes to shared memory
-// in a transposed layout (`red`: kPartFields x blockDim doubles; it may
-// alias buffers the block used for the tile, the first barrier retires
-// them).  Warp w reduces fields w, w + nwarps, ... (each lane folds its
-// column in a fixed order, then a fixed shuffle tree) and writes them into
-// the tile's record.  Nothing more happens at the tile's end: the next node
-// pass folds the records (fold_field), so no tile waits for a fence or an
-// atomic.  The last barrier retires `red` for the next tile of a
-// persistent block.
-template <bool FIELD_MAJOR>
+// The tile's reduction record.  Every thread's Part goes to shared memory in
+// a transposed layout (`red`: kPartFields rows of blockDim doubles).  With
+// ALIASED, `red` overlays buffers the block used for the tile, so a barrier
+// retires them first; a buffer of the block's own needs none.  Then the
+// fields are reduced all at once, blockDim/16 threads a field (224 of 256):
+// thread i of field f's group loads the group's values i, i + blockDim/16,
+// ... (16 of them), folds them as a fixed binary tree, and the group folds
+// its partials with a fixed shuffle tree -- eight dependent levels, where
+// one warp folding its fields one after another took about 24.  The record
+// is written by each group's first thread.  Nothing more happens at the
+// tile's end: the next node pass folds the records (fold_field), so no tile
+// waits for a fence or an atomic.  The last barrier retires `red` for the
+// next tile of a persistent block.
+template <bool FIELD_MAJOR, bool ALIASED>
 __device__ __forceinline__ void tile_record(const DevMesh &m, const DevState &s, int64_t tile, const Part &p,
                                             double *red) {
-    const int B = blockDim.x, t = threadIdx.x, lane = t & 31, warp = t >> 5, nw = B >> 5;
-    __syncthreads();
+    const int B = blockDim.x, t = threadIdx.x;
+    const int tpf = B >> 4;  // threads per field (16 values each); B is a multiple of 32, at most 256
+    if (ALIASED) __syncthreads();
     p.store_strided(red + t, B);
     __syncthreads();
-    for (int f = warp; f < kPartFields; f += nw) {
-        const double *row = red + f * B;
-        double x = row[lane];
-        for (int j = lane + 32; j < B; j += 32) x = part_op(f, x, row[j]);
-        for (int off = 16; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, off));
-        if (lane == 0) *part_at<FIELD_MAJOR>(m, s, tile, f) = x;
+    const int f = t / tpf, i = t - f * tpf;
+    if (f < kPartFields) {
+        const double *row = red + f * B + i;
+        double v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = row[k * tpf];
+#pragma unroll
+        for (int h = 8; h > 0; h >>= 1)
+#pragma unroll
+            for (int k = 0; k < h; ++k) v[k] = part_op(f, v[k], v[k + h]);
+        double x = v[0];
+        // a group's lanes are consecutive within one warp (tpf <= 16); the
+        // lanes of this warp below thread kPartFields * tpf take part
+        const int lim = kPartFields * tpf - (t & ~31);
+        const unsigned mask = lim >= 32 ? 0xffffffffu : ((1u << lim) - 1u);
+        for (int off = tpf >> 1; off > 0; off >>= 1) x = part_op(f, x, __shfl_down_sync(mask, x, off, tpf));
+        if (i == 0) *part_at<FIELD_MAJOR>(m, s, tile, f) = x;
     }
     __syncthreads();
 }
@@ -514,7 +530,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step(const DevMesh m, const 
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update(m, s, P, g, me, F, diff, dt, load_cell_in(m, s, g), pout, part);
         }
-        tile_record<true>(m, s, tile, part, s_red);
+        tile_record<true, false>(m, s, tile, part, s_red);
     }
 }
 
@@ -539,7 +555,6 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
     static_assert((1 + NS) * 256 * 4 >= kPartFields * 256, "reduction buffer");
     double4 *const s_prim = s_mem;
     double4 (*const s_flux)[256] = reinterpret_cast<double4 (*)[256]>(s_mem + 256);
-    double *const s_red = reinterpret_cast<double *>(s_mem);
     pdl_trigger();
     pdl_wait();
     const int par = *s.parity;
@@ -634,7 +649,7 @@ __global__ void __launch_bounds__(256, MINB) k_cell_step_tf(const DevMesh m, con
             }
             cell_update(m, s, P, g, me, F, diff, dt, cin, pout, part);
         }
-        tile_record<true>(m, s, tile, part, s_red);
+        tile_record<true, true>(m, s, tile, part, reinterpret_cast<double *>(s_mem));
     }
 }
 
@@ -837,7 +852,7 @@ static __global__ void __launch_bounds__(256) k_init_state(const DevMesh m, cons
             part.vmax = vmax;
             part.rmin = m.charlen[g] / vmax;
         }
-        tile_record<true>(m, s, tile, part, s_red);
+        tile_record<true, false>(m, s, tile, part, s_red);
     }
 }
 
@@ -928,7 +943,7 @@ __global__ void __launch_bounds__(256, MINB) k_face_update(const DevMesh m, cons
             if (VISC) diff_source<QUAD>(m, s, P, g, is_quad, me, diff);
             cell_update(m, s, P, g, me, F, diff, dt, load_cell_in(m, s, g), pout, part);
         }
-        tile_record<true>(m, s, tile, part, s_red);
+        tile_record<true, false>(m, s, tile, part, s_red);
     }
 }
 
