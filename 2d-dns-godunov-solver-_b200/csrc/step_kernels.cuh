@@ -191,38 +191,38 @@ __device__ __forceinline__ double *part_at(const DevMesh &m, const DevState &s, 
     return FIELD_MAJOR ? s.part + (int64_t)f * m.ntiles + q : s.part + q * kPartials + f;
 }
 
-// The tile's reduction record.  Every thread's Part goes to shared memory in
-// a transposed layout (`red`: kPartFields rows of blockDim doubles).  With
-// ALIASED, `red` overlays buffers the block used for the tile, so a barrier
-// retires them first; a buffer of the block's own needs none.  Then the
-// fields are reduced all at once, blockDim/16 threads a field (224 of 256):
-// thread i of field f's group loads the group's values i, i + blockDim/16,
-// ... (16 of them), folds them as a fixed binary tree, and the group folds
-// its partials with a fixed shuffle tree -- eight dependent levels, where
-// one warp folding its fields one after another took about 24.  The record
-// is written by each group's first thread.  Nothing more happens at the
-// tile's end: the next node pass folds the records (fold_field), so no tile
-// waits for a fence or an atomic.  The last barrier retires `red` for the
-// next tile of a persistent block.
+// The tile's reduction record.  With ALIASED, the staging buffer `red`
+// overlays buffers the block used for the tile, so a barrier retires them
+// first; a buffer of the block's own needs none.  Each field is folded in a
+// fixed order: two shuffle levels over groups of four lanes (so a quarter
+// of the values go through shared memory: `red` holds kPartFields rows of
+// blockDim/4), then blockDim/16 threads a field (224 of 256) fold four
+// values each and a fixed shuffle tree joins them -- eight dependent levels
+// in all.  The record is written by each field group's first thread.
+// Nothing more happens at the tile's end: the next node pass folds the
+// records (fold_field), so no tile waits for a fence or an atomic.  The
+// last barrier retires `red` for the next tile of a persistent block.
 template <bool FIELD_MAJOR, bool ALIASED>
 __device__ __forceinline__ void tile_record(const DevMesh &m, const DevState &s, int64_t tile, const Part &p,
                                             double *red) {
-    const int B = blockDim.x, t = threadIdx.x;
-    const int tpf = B >> 4;  // threads per field (16 values each); B is a multiple of 32, at most 256
+    const int B = blockDim.x, t = threadIdx.x, lane = t & 31;
+    const int R = B >> 2;    // values per field after the lane folds
+    const int tpf = B >> 4;  // threads per field (4 values each); B is 128 or 256
     if (ALIASED) __syncthreads();
-    p.store_strided(red + t, B);
+    const double v[kPartFields] = {p.res[0], p.res[1], p.res[2], p.res[3], p.tot[0], p.tot[1], p.tot[2],
+                                   p.tot[3], p.ek, p.vmax, p.rmin, p.rhomin, p.rhomax, p.bad};
+#pragma unroll
+    for (int f = 0; f < kPartFields; ++f) {
+        double x = v[f];
+        x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, 1));
+        x = part_op(f, x, __shfl_down_sync(0xffffffffu, x, 2));
+        if ((lane & 3) == 0) red[f * R + (t >> 2)] = x;
+    }
     __syncthreads();
     const int f = t / tpf, i = t - f * tpf;
     if (f < kPartFields) {
-        const double *row = red + f * B + i;
-        double v[16];
-#pragma unroll
-        for (int k = 0; k < 16; ++k) v[k] = row[k * tpf];
-#pragma unroll
-        for (int h = 8; h > 0; h >>= 1)
-#pragma unroll
-            for (int k = 0; k < h; ++k) v[k] = part_op(f, v[k], v[k + h]);
-        double x = v[0];
+        const double *row = red + f * R + i;
+        double x = part_op(f, part_op(f, row[0], row[tpf]), part_op(f, row[2 * tpf], row[3 * tpf]));
         // a group's lanes are consecutive within one warp (tpf <= 16); the
         // lanes of this warp below thread kPartFields * tpf take part
         const int lim = kPartFields * tpf - (t & ~31);
