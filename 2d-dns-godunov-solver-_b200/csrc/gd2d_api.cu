@@ -1023,22 +1023,26 @@ static void stage_copy(double *stage, double *const cols[4], int64_t n, size_t b
     }
 }
 
-// Whether a host buffer is page-locked in the current context (allocated
-// or registered with CUDA), so that the copy engine can read or write it
-// directly.  Pageable memory is not an error.
-static bool host_pinned(const void *p) {
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        (void)cudaGetLastError();
-        return false;
+// Whether a host array of n doubles is page-locked in the current context
+// (allocated or registered with CUDA), first and last element alike, so
+// that the copy engine can read or write it directly.  Pageable memory is
+// not an error.
+static bool host_pinned(const double *p, int64_t n) {
+    for (const double *q : {p, p + (n > 0 ? n - 1 : 0)}) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+            (void)cudaGetLastError();
+            return false;
+        }
+        if (a.type != cudaMemoryTypeHost) return false;
     }
-    return a.type == cudaMemoryTypeHost;
+    return true;
 }
 
 // Host columns -> h_stage -> d_stage (queued on the handle's stream).
 // Page-locked columns are copied to d_stage directly.
 static int staged_upload(gd2d_handle *h, const double *const src[4], int64_t n) {
-    if (host_pinned(src[0]) && host_pinned(src[1]) && host_pinned(src[2]) && host_pinned(src[3])) {
+    if (host_pinned(src[0], n) && host_pinned(src[1], n) && host_pinned(src[2], n) && host_pinned(src[3], n)) {
         for (int v = 0; v < 4; ++v) {
             const cudaError_t e = cudaMemcpyAsync(h->d_stage + (size_t)v * n, src[v], sizeof(double) * (size_t)n,
                                                   cudaMemcpyHostToDevice, h->stream);
@@ -1066,7 +1070,7 @@ static int staged_upload(gd2d_handle *h, const double *const src[4], int64_t n) 
 // matrix is complete.  A page-locked matrix is copied to directly.
 static int staged_download(gd2d_handle *h, double *dst, int64_t n) {
     const size_t total = 4 * (size_t)n;
-    if (host_pinned(dst)) {
+    if (host_pinned(dst, (int64_t)total)) {
         cudaError_t e = cudaMemcpyAsync(dst, h->d_stage, sizeof(double) * total, cudaMemcpyDeviceToHost, h->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) {
