@@ -64,17 +64,6 @@ struct Part {
         rhomax = fmax(rhomax, o.rhomax);
         bad = fmax(bad, o.bad);
     }
-    // field f at p[f * stride], in record order
-    __device__ void store_strided(double *p, int stride) const {
-        for (int v = 0; v < 4; ++v) { p[(P_RES0 + v) * stride] = res[v]; p[(P_TOT0 + v) * stride] = tot[v]; }
-        p[P_EK * stride] = ek; p[P_VMAX * stride] = vmax; p[P_RMIN * stride] = rmin;
-        p[P_RHOMIN * stride] = rhomin; p[P_RHOMAX * stride] = rhomax; p[P_BAD * stride] = bad;
-    }
-    __device__ void store(double *p) const {
-        for (int v = 0; v < 4; ++v) { p[P_RES0 + v] = res[v]; p[P_TOT0 + v] = tot[v]; }
-        p[P_EK] = ek; p[P_VMAX] = vmax; p[P_RMIN] = rmin; p[P_RHOMIN] = rhomin; p[P_RHOMAX] = rhomax;
-        p[P_BAD] = bad;
-    }
     __device__ void load_cg(const double *p) {
         for (int v = 0; v < 4; ++v) { res[v] = __ldcg(p + P_RES0 + v); tot[v] = __ldcg(p + P_TOT0 + v); }
         ek = __ldcg(p + P_EK); vmax = __ldcg(p + P_VMAX); rmin = __ldcg(p + P_RMIN);
