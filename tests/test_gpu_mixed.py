@@ -76,7 +76,7 @@ def test_mixed_cylinder_1000_steps_against_fp64(pkg):
     for prec in ("f64", "mixed"):
         s = pkg.setupSolver(mesh, cfg, precision=prec, loop="tile")
         s.createFields2d(0, *prims)
-        h = s.propagate2d(1000)
+        s.propagate2d(1000)
         out[prec] = s.get_state(0)["Ucons"]
         assert all(x["nonfinite"] == 0 for x in s.history(0)), prec
         s.close()
